@@ -1,0 +1,911 @@
+// Host engine of the HOS time-advance library: handle lifetime, device
+// buffers, the per-stage pass sequence, CUDA-graph capture of a step, and the
+// handle C ABI declared in include/hos_gpu.h.
+//
+// One RHS evaluation (rhs_hos, hosm_2d_par.c:138-235, with Zvel,
+// hosm_2d_par.c:240-445) is issued as
+//   xinv  : stage input u + dt*sum b k, i kx / z-derivative multipliers, x-inverse
+//   yinv  : y-inverse -> eta, eta_x, eta_y, phi_x, phi_y, d_z^j phi^(1)
+//   for n = 1..M-1 (Taylor levels of the W recursion):
+//     yfwd  : P_n = -sum_m d_z^(n-m) phi^(m+1) eta^(n-m)/(n-m)!, y-forward
+//     xfwd  : x-forward (-> phi^(n+1) hat), then z-derivative multipliers, x-inverse
+//     yinv  : y-inverse -> d_z^j phi^(n+1), epilogue W_n
+//   yfwd  : RHS assembly in physical space, y-forward (rows ky < my only)
+//   xfwd  : x-forward, + Dz phi / - g eta, ramp, dealias, k_s, Hamiltonian,
+//           final RK update on the last stage
+// Every product the reference forms with Mult (operators_par.c:210-235) is a
+// pointwise product of fields that both designs obtain through the same c2r,
+// so the restructuring changes only the rounding.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "hos_gpu.h"
+#include "hos_registry.h"
+
+namespace hos {
+XInvFn lookup_xinv_64(int n);
+XFwdFn lookup_xfwd_64(int n);
+YInvFn lookup_yinv_64(int h);
+YFwdFn lookup_yfwd_64(int h);
+XInvFn lookup_xinv_32(int n);
+XFwdFn lookup_xfwd_32(int n);
+YInvFn lookup_yinv_32(int h);
+YFwdFn lookup_yfwd_32(int h);
+XInvFn lookup_xinv(int prec, int n) { return prec ? lookup_xinv_32(n) : lookup_xinv_64(n); }
+XFwdFn lookup_xfwd(int prec, int n) { return prec ? lookup_xfwd_32(n) : lookup_xfwd_64(n); }
+YInvFn lookup_yinv(int prec, int h) { return prec ? lookup_yinv_32(h) : lookup_yinv_64(h); }
+YFwdFn lookup_yfwd(int prec, int h) { return prec ? lookup_yfwd_32(h) : lookup_yfwd_64(h); }
+
+// ---------------------------------------------------------------- small kernels
+__global__ void k_set_int(int* p, int v) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *p = v;
+}
+
+// Active rows of the packed state: 1 + the largest ky row holding a nonzero
+// (or non-finite) value in either field, at least `lo`.
+__global__ void k_active_rows(const double2* u, size_t fsz, int nx, int row0, int* act) {
+  const int row = row0 + blockIdx.x;
+  int any = 0;
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+    const double2 a = u[(size_t)row * nx + i];
+    const double2 b = u[fsz + (size_t)row * nx + i];
+    if (a.x != 0.0 || a.y != 0.0 || b.x != 0.0 || b.y != 0.0) any = 1;
+  }
+  any = __syncthreads_or(any);
+  if (any && threadIdx.x == 0) atomicMax(act, row + 1);
+}
+
+__global__ void k_nonfinite(const double2* u, size_t n, int* flag) {
+  int bad = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double2 a = u[i];
+    if (!isfinite(a.x) || !isfinite(a.y)) bad = 1;
+  }
+  bad = __syncthreads_or(bad);
+  if (bad && threadIdx.x == 0) atomicOr(flag, 1);
+}
+
+// ---------------------------------------------------------------- step end
+// Sums the stage-0 Hamiltonian partials in a fixed order, records (t, H) and
+// advances t (time_schemes_par.c:73-93,119).
+__global__ void k_step_end(const double* ham_part, int nparts, double* tdev, double dt, long long* stepdev,
+                           double* ham_hist, double* t_hist, int hist_cap) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double s = 0.0;
+  for (int i = 0; i < nparts; i++) s += ham_part[i];
+  const long long st = *stepdev;
+  if (st >= 0) {  // ring of hist_cap records
+    ham_hist[st % hist_cap] = s;
+    t_hist[st % hist_cap] = *tdev;
+  }
+  *tdev = *tdev + dt;
+  *stepdev = st + 1;
+}
+
+}  // namespace hos
+
+using namespace hos;
+
+// ---------------------------------------------------------------- errors
+static thread_local std::string g_err;
+
+static int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define HOS_CK(x)                                                                                  \
+  do {                                                                                             \
+    cudaError_t e_ = (x);                                                                          \
+    if (e_ != cudaSuccess) {                                                                       \
+      (void)cudaGetLastError();                                                                    \
+      return fail(e_ == cudaErrorMemoryAllocation ? HOS_ERR_NOMEM : HOS_ERR_CUDA, "%s: %s", #x,    \
+                  cudaGetErrorString(e_));                                                         \
+    }                                                                                              \
+  } while (0)
+
+// ---------------------------------------------------------------- plan
+namespace {
+
+struct PassCfg {
+  XInvFn xinv = nullptr;
+  XFwdFn xfwd = nullptr;
+  YInvFn yinv = nullptr;
+  YFwdFn yfwd = nullptr;
+  int xlines = 1, xthreads = 0;
+  size_t xsmem = 0;
+  int ylines = 1, ythreads = 0, ytp = 0;
+  size_t ysmem = 0;
+  const void* tw = nullptr;
+};
+
+int ilog2i(int n) {
+  int r = 0;
+  while ((1 << r) < n) r++;
+  return r;
+}
+
+bool pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+// Butcher tables of Setup_TimeScheme (time_schemes_par.c:127-314).
+int butcher(int scheme, int* nst, double b[MAX_STAGES][MAX_STAGES], double c[MAX_STAGES]) {
+  for (int i = 0; i < MAX_STAGES; i++) {
+    c[i] = 0.0;
+    for (int j = 0; j < MAX_STAGES; j++) b[i][j] = 0.0;
+  }
+  switch (scheme) {
+    case HOS_RK45DP:
+      *nst = 7;
+      b[1][0] = 1.0 / 5.0;
+      b[2][0] = 3.0 / 40.0;
+      b[3][0] = 44.0 / 45.0;
+      b[4][0] = 19372.0 / 6561.0;
+      b[5][0] = 9017.0 / 3168.0;
+      b[6][0] = 35.0 / 384.0;
+      b[2][1] = 9.0 / 40.0;
+      b[3][1] = -56.0 / 15.0;
+      b[4][1] = -25360.0 / 2187.0;
+      b[5][1] = -355.0 / 33.0;
+      b[6][1] = 0.0;
+      b[3][2] = 32.0 / 9.0;
+      b[4][2] = 64448.0 / 6561.0;
+      b[5][2] = 46732.0 / 5247.0;
+      b[6][2] = 500.0 / 1113.0;
+      b[4][3] = -212.0 / 729.0;
+      b[5][3] = 49.0 / 176.0;
+      b[6][3] = 125.0 / 192.0;
+      b[5][4] = -5103.0 / 18656.0;
+      b[6][4] = -2187.0 / 6784.0;
+      b[6][5] = 11.0 / 84.0;
+      c[0] = 1951.0 / 21600.0;
+      c[1] = 0.0;
+      c[2] = 22642.0 / 50085.0;
+      c[3] = 451.0 / 720.0;
+      c[4] = -12231.0 / 42400.0;
+      c[5] = 649.0 / 6300.0;
+      c[6] = 1.0 / 60.0;
+      return 0;
+    case HOS_RK4:
+      *nst = 4;
+      b[1][0] = 0.5;
+      b[2][1] = 0.5;
+      b[3][2] = 1.0;
+      c[0] = 1.0 / 6.0;
+      c[1] = 1.0 / 3.0;
+      c[2] = 1.0 / 3.0;
+      c[3] = 1.0 / 6.0;
+      return 0;
+    case HOS_EULER:
+      *nst = 1;
+      c[0] = 1.0;
+      return 0;
+    case HOS_MIDPOINT:
+      *nst = 2;
+      b[1][0] = 0.5;
+      c[0] = 0.0;
+      c[1] = 1.0;
+      return 0;
+    case HOS_HEUN:
+      *nst = 2;
+      b[1][0] = 1.0;
+      c[0] = 0.5;
+      c[1] = 0.5;
+      return 0;
+    default:
+      return -1;
+  }
+}
+
+// exp(-2 pi i k / TW_N), k < TW_N, from long double libm, rounded once.
+std::vector<double2> twiddle_table() {
+  std::vector<double2> t(TW_N);
+  const long double pi = 3.141592653589793238462643383279502884L;
+  for (int k = 0; k < TW_N; k++) {
+    const long double a = 2.0L * pi * (long double)k / (long double)TW_N;
+    t[k].x = (double)cosl(a);
+    t[k].y = (double)-sinl(a);
+  }
+  return t;
+}
+
+constexpr int HIST_CAP = 1 << 16;
+
+}  // namespace
+
+struct hos_ctx {
+  hos_params p{};
+  int nx = 0, ny = 0, h = 0, M = 0, L = 0, prec = 0;
+  Geo geo{};
+  int nst = 0;
+  double b[MAX_STAGES][MAX_STAGES]{};
+  double c[MAX_STAGES]{};
+  size_t fsz = 0, psz = 0;
+  int nz = 0, nphys = 0;
+  // device memory
+  double2* u = nullptr;
+  double2* k = nullptr;
+  void* zbuf = nullptr;
+  void* phys = nullptr;
+  double2* ustage = nullptr;
+  double2* zplain = nullptr;
+  double* pplain = nullptr;
+  double2* tw64 = nullptr;
+  float2* tw32 = nullptr;
+  double* tdev = nullptr;
+  double* trhs = nullptr;
+  double* rdev = nullptr;
+  long long* stepdev = nullptr;
+  int* actdev = nullptr;
+  int* flagdev = nullptr;
+  double* ham_part = nullptr;
+  int nparts = 0;
+  double* ham_hist = nullptr;
+  double* t_hist = nullptr;
+  long long hist_base = 0;
+  cudaStream_t st = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  double g_dt = 0.0;
+  bool g_valid = false;
+  PassCfg cfg;    // compute precision
+  PassCfg cfg64;  // FP64 passes for the boundary transforms
+  int device = 0;
+
+  // physical field indices
+  int ETA() const { return 0; }
+  int ETAX() const { return 1; }
+  int ETAY() const { return 2; }
+  int PHIX() const { return 3; }
+  int PHIY() const { return 4; }
+  // d_z^j phi^(i), i = 1..M, j = 1..M+1-i
+  int D(int i, int j) const {
+    int off = 5;
+    for (int q = 1; q < i; q++) off += M + 1 - q;
+    return off + (j - 1);
+  }
+  // W_n, n = 1..L (W_0 = D(1,1))
+  int W(int n) const { return n == 0 ? D(1, 1) : 5 + M * (M + 1) / 2 + (n - 1); }
+};
+
+namespace {
+
+int make_cfg(hos_ctx* c, int prec, PassCfg* o) {
+  o->xinv = lookup_xinv(prec, c->nx);
+  o->xfwd = lookup_xfwd(prec, c->nx);
+  o->yinv = lookup_yinv(prec, c->h);
+  o->yfwd = lookup_yfwd(prec, c->h);
+  if (!o->xinv || !o->xfwd || !o->yinv || !o->yfwd) return fail(HOS_ERR_ARG, "no kernels for %dx%d", c->nx, c->ny);
+  const size_t cs = prec ? sizeof(float2) : sizeof(double2);
+  {
+    const int E = elems_for(c->nx), P = c->nx / E;
+    int lines = MAX_THREADS / P;
+    if (lines < 1) lines = 1;
+    o->xlines = lines;
+    o->xthreads = lines * P;
+    o->xsmem = (size_t)lines * (size_t)(c->nx + c->nx / E) * cs;
+  }
+  {
+    const int E = elems_for(c->h), P = c->h / E;
+    int lines = MAX_THREADS / P;
+    if (lines > c->nx) lines = c->nx;
+    if (lines < 1) lines = 1;
+    o->ylines = lines;
+    o->ythreads = lines * P;
+    const int phase = (int)(128 / cs);
+    const int target = lines >= phase ? 1 : phase / lines;
+    int tp = c->h + 1;
+    while (tp % phase != target % phase) tp++;
+    o->ytp = tp;
+    o->ysmem = ((size_t)lines * tp + (size_t)lines * (c->h + c->h / E)) * cs;
+  }
+  if (o->xthreads % 32 != 0) return fail(HOS_ERR_ARG, "x-pass block of %d threads", o->xthreads);
+  HOS_CK(cudaFuncSetAttribute((const void*)o->xinv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->xsmem));
+  HOS_CK(cudaFuncSetAttribute((const void*)o->xfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->xsmem));
+  HOS_CK(cudaFuncSetAttribute((const void*)o->yinv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->ysmem));
+  HOS_CK(cudaFuncSetAttribute((const void*)o->yfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->ysmem));
+  o->tw = prec ? (const void*)c->tw32 : (const void*)c->tw64;
+  return HOS_OK;
+}
+
+inline int xgrid(const hos_ctx* c, const PassCfg& g) { return (c->h + 1 + g.xlines - 1) / g.xlines; }
+inline int ygrid(const hos_ctx* c, const PassCfg& g) { return c->nx / g.ylines; }
+
+size_t compute_bytes(const hos_params* p, int nst) {
+  const size_t nx = p->nx, ny = p->ny, h = ny / 2;
+  const size_t fsz = (h + 1) * nx, psz = nx * ny;
+  const int M = p->order, L = M - 1;
+  const size_t cs = p->precision ? 8 : 16, rs = p->precision ? 4 : 8;
+  size_t b = 0;
+  b += 2 * fsz * 16;                                 // u
+  b += (size_t)nst * 2 * fsz * 16;                   // k
+  b += (size_t)(4 + M) * fsz * cs;                   // Z / V scratch
+  b += (size_t)(5 + M * (M + 1) / 2 + L) * psz * rs; // physical fields
+  b += 2 * fsz * 16 + fsz * 16 + 2 * psz * 8;        // boundary scratch (FP64)
+  b += (size_t)TW_N * (16 + 8);
+  b += 2 * (size_t)HIST_CAP * 8 + 4096 * 8 + 4096;
+  return b;
+}
+
+// Enqueues one RK stage (or one bare RHS evaluation when rhs_only).
+int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, double2* kout, const double* tsrc,
+                  const int* rows_dev) {
+  const PassCfg& g = c->cfg;
+  const int M = c->M, L = c->L;
+  const size_t fsz = c->fsz;
+  const size_t cs = c->prec ? sizeof(float2) : sizeof(double2);
+  char* zb = reinterpret_cast<char*>(c->zbuf);
+
+  XInvArgs xa{};
+  xa.geo = c->geo;
+  xa.mode = 0;
+  xa.rows = c->h + 1;
+  xa.rows_dev = rows_dev;
+  xa.u = uin;
+  int nk = 0;
+  for (int p = 0; p < s; p++) {
+    if (c->b[s][p] != 0.0) {
+      xa.kp[nk] = c->k + (size_t)p * 2 * fsz;
+      xa.coef[nk] = dt * c->b[s][p];
+      nk++;
+    }
+  }
+  xa.nk = nk;
+  xa.ndz = M;
+  xa.z = c->zbuf;
+  xa.tdev = tsrc;
+  xa.rdev = c->rdev;
+  xa.set_ramp = (s == 0);
+  xa.tramp = c->p.tramp;
+  xa.rampflg = c->p.rampflg;
+  g.xinv<<<xgrid(c, g), g.xthreads, g.xsmem, c->st>>>(xa, g.tw);
+
+  YInvArgs ya{};
+  ya.geo = c->geo;
+  ya.tp = g.ytp;
+  ya.z = c->zbuf;
+  ya.rows_in = c->h + 1;
+  ya.rows_dev = rows_dev;
+  ya.phys = c->phys;
+  int nj = 0;
+  ya.jobs[nj++] = YJob{0, 0, c->ETA()};
+  ya.jobs[nj++] = YJob{0, 1, c->ETAY()};
+  ya.jobs[nj++] = YJob{1, 0, c->ETAX()};
+  ya.jobs[nj++] = YJob{2, 1, c->PHIY()};
+  ya.jobs[nj++] = YJob{3, 0, c->PHIX()};
+  for (int j = 1; j <= M; j++) ya.jobs[nj++] = YJob{4 + j - 1, 0, c->D(1, j)};
+  ya.njobs = nj;
+  ya.wmode = 0;
+  g.yinv<<<ygrid(c, g), g.ythreads, g.ysmem, c->st>>>(ya, g.tw);
+
+  for (int n = 1; n <= L; n++) {
+    YFwdArgs fa{};
+    fa.geo = c->geo;
+    fa.tp = g.ytp;
+    fa.mode = 1;
+    fa.phys = c->phys;
+    fa.eta = c->ETA();
+    fa.nterms = n;
+    for (int m = 0; m < n; m++) {
+      fa.t_in[m] = c->D(m + 1, n - m);
+      fa.t_pow[m] = n - m;
+    }
+    fa.vout = zb;
+    fa.rows_out = c->h + 1;
+    g.yfwd<<<ygrid(c, g), g.ythreads, g.ysmem, c->st>>>(fa, g.tw);
+
+    XFwdArgs xf{};
+    xf.geo = c->geo;
+    xf.mode = 1;
+    xf.rows = c->h + 1;
+    xf.vin0 = zb;
+    xf.zout = zb + fsz * cs;
+    xf.ndz = M - n;
+    g.xfwd<<<xgrid(c, g), g.xthreads, g.xsmem, c->st>>>(xf, g.tw);
+
+    YInvArgs yl{};
+    yl.geo = c->geo;
+    yl.tp = g.ytp;
+    yl.z = c->zbuf;
+    yl.rows_in = c->h + 1;
+    yl.phys = c->phys;
+    int nl = 0;
+    for (int j = 1; j <= M - n; j++) yl.jobs[nl++] = YJob{1 + j - 1, 0, c->D(n + 1, j)};
+    yl.njobs = nl;
+    yl.wmode = 1;
+    yl.w_out = c->W(n);
+    yl.eta = c->ETA();
+    yl.w_terms = n;
+    for (int m = 0; m < n; m++) {
+      yl.w_in[m] = c->D(m + 1, n - m + 1);
+      yl.w_pow[m] = n - m;
+    }
+    g.yinv<<<ygrid(c, g), g.ythreads, g.ysmem, c->st>>>(yl, g.tw);
+  }
+
+  YFwdArgs ff{};
+  ff.geo = c->geo;
+  ff.tp = g.ytp;
+  ff.mode = 2;
+  ff.phys = c->phys;
+  ff.ex = c->ETAX();
+  ff.ey = c->ETAY();
+  ff.px = c->PHIX();
+  ff.py = c->PHIY();
+  ff.L = L;
+  for (int n = 0; n <= L; n++) ff.w_idx[n] = c->W(n);
+  ff.vout = zb;
+  ff.rows_out = c->geo.my;
+  g.yfwd<<<ygrid(c, g), g.ythreads, g.ysmem, c->st>>>(ff, g.tw);
+
+  XFwdArgs xe{};
+  xe.geo = c->geo;
+  xe.mode = 2;
+  xe.rows = c->h + 1;
+  xe.rows_dev = rows_dev;
+  xe.rows_fft = c->geo.my;
+  xe.vin0 = zb;
+  xe.vin1 = zb + fsz * cs;
+  xe.u = uin;
+  for (int p = 0; p < nk; p++) {
+    xe.kp[p] = xa.kp[p];
+    xe.coef[p] = xa.coef[p];
+  }
+  xe.nk = nk;
+  xe.kout = kout;
+  xe.rdev = c->rdev;
+  xe.ham = (!rhs_only && s == 0);
+  xe.ham_part = c->ham_part;
+  xe.final_update = (!rhs_only && s == c->nst - 1);
+  for (int p = 0; p < c->nst; p++) {
+    xe.kall[p] = c->k + (size_t)p * 2 * fsz;
+    xe.cfin[p] = dt * c->c[p];
+  }
+  xe.nstage = c->nst;
+  xe.unew = uin;
+  g.xfwd<<<xgrid(c, g), g.xthreads, g.xsmem, c->st>>>(xe, g.tw);
+  return HOS_OK;
+}
+
+int enqueue_step(hos_ctx* c, double dt) {
+  for (int s = 0; s < c->nst; s++) {
+    int rc = enqueue_stage(c, s, dt, false, c->u, c->k + (size_t)s * 2 * c->fsz, c->tdev, c->actdev);
+    if (rc) return rc;
+  }
+  k_step_end<<<1, 32, 0, c->st>>>(c->ham_part, xgrid(c, c->cfg), c->tdev, dt, c->stepdev, c->ham_hist, c->t_hist,
+                                  HIST_CAP);
+  return HOS_OK;
+}
+
+int build_graph(hos_ctx* c, double dt) {
+  if (c->g_valid && c->g_dt == dt) return HOS_OK;
+  if (c->gexec) {
+    cudaGraphExecDestroy(c->gexec);
+    c->gexec = nullptr;
+  }
+  if (c->graph) {
+    cudaGraphDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  c->g_valid = false;
+  HOS_CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+  int rc = enqueue_step(c, dt);
+  cudaGraph_t gr = nullptr;
+  cudaError_t e = cudaStreamEndCapture(c->st, &gr);
+  if (rc) {
+    if (gr) cudaGraphDestroy(gr);
+    return rc;
+  }
+  HOS_CK(e);
+  c->graph = gr;
+  HOS_CK(cudaGraphInstantiate(&c->gexec, c->graph, 0));
+  c->g_dt = dt;
+  c->g_valid = true;
+  return HOS_OK;
+}
+
+// Plain FP64 transforms used at the boundary.
+int enqueue_r2c(hos_ctx* c, const double* phys_in, double2* spec_out, int dealias) {
+  const PassCfg& g = c->cfg64;
+  YFwdArgs fa{};
+  fa.geo = c->geo;
+  fa.tp = g.ytp;
+  fa.mode = 0;
+  fa.in_ptr = phys_in;
+  fa.vout = c->zplain;
+  fa.rows_out = c->h + 1;
+  g.yfwd<<<ygrid(c, g), g.ythreads, g.ysmem, c->st>>>(fa, g.tw);
+  XFwdArgs xf{};
+  xf.geo = c->geo;
+  xf.mode = 0;
+  xf.rows = c->h + 1;
+  xf.vin0 = c->zplain;
+  xf.out_spec = spec_out;
+  xf.dealias = dealias;
+  g.xfwd<<<xgrid(c, g), g.xthreads, g.xsmem, c->st>>>(xf, g.tw);
+  return HOS_OK;
+}
+
+int enqueue_c2r(hos_ctx* c, const double2* spec_in, double* phys_out) {
+  const PassCfg& g = c->cfg64;
+  XInvArgs xa{};
+  xa.geo = c->geo;
+  xa.mode = 1;
+  xa.rows = c->h + 1;
+  xa.u = spec_in;
+  xa.z = c->zplain;
+  xa.tdev = c->tdev;
+  xa.rdev = c->rdev;
+  xa.set_ramp = 0;
+  g.xinv<<<xgrid(c, g), g.xthreads, g.xsmem, c->st>>>(xa, g.tw);
+  YInvArgs ya{};
+  ya.geo = c->geo;
+  ya.tp = g.ytp;
+  ya.z = c->zplain;
+  ya.rows_in = c->h + 1;
+  ya.phys = phys_out;
+  ya.jobs[0] = YJob{0, 0, 0};
+  ya.njobs = 1;
+  g.yinv<<<ygrid(c, g), g.ythreads, g.ysmem, c->st>>>(ya, g.tw);
+  return HOS_OK;
+}
+
+int refresh_active_rows(hos_ctx* c, const double2* u, int* act) {
+  k_set_int<<<1, 32, 0, c->st>>>(act, c->geo.my);
+  const int from = c->geo.my;
+  if (from < c->h + 1) k_active_rows<<<c->h + 1 - from, 128, 0, c->st>>>(u, c->fsz, c->nx, from, act);
+  return HOS_OK;
+}
+
+void release(hos_ctx* c) {
+  if (!c) return;
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  if (c->graph) cudaGraphDestroy(c->graph);
+  void* ptrs[] = {c->u,      c->k,    c->zbuf, c->phys,    c->ustage, c->zplain, c->pplain,   c->tw64,
+                  c->tw32,   c->tdev, c->trhs, c->rdev,    c->stepdev, c->actdev, c->flagdev, c->ham_part,
+                  c->ham_hist, c->t_hist};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+}
+
+template <typename P>
+int dalloc(P** p, size_t bytes) {
+  cudaError_t e = cudaMalloc((void**)p, bytes ? bytes : 16);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    *p = nullptr;
+    return fail(e == cudaErrorMemoryAllocation ? HOS_ERR_NOMEM : HOS_ERR_CUDA, "cudaMalloc(%zu): %s", bytes,
+                cudaGetErrorString(e));
+  }
+  return HOS_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- C ABI
+extern "C" {
+
+void hos_default_params(hos_params* p, int nx, int ny) {
+  std::memset(p, 0, sizeof(*p));
+  p->nx = nx;
+  p->ny = ny;
+  p->lx = 2 * M_PI;
+  p->ly = 2 * M_PI;
+  p->g = 1.0;
+  p->order = 3;
+  p->precision = HOS_PREC_FP64;
+  p->depth = 0.0;
+  p->rampflg = 0;
+  p->tramp = 1.0;
+  p->scheme = HOS_RK4;
+  p->mx = 0;
+  p->my = 0;
+}
+
+const char* hos_last_error(void) { return g_err.c_str(); }
+
+const char* hos_version(void) {
+  return "hos_b200 sm_100a: Stockham line FFT passes (radix-8/16), fused HOS RHS, FP64/FP32 compute";
+}
+
+size_t hos_footprint_bytes(const hos_params* p) {
+  if (!p) return 0;
+  int nst = 0;
+  double b[MAX_STAGES][MAX_STAGES], c[MAX_STAGES];
+  if (butcher(p->scheme, &nst, b, c)) return 0;
+  return compute_bytes(p, nst);
+}
+
+int hos_create(const hos_params* p, hos_handle* out) {
+  if (!p || !out) return fail(HOS_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (!pow2(p->nx) || !pow2(p->ny) || p->nx < 16 || p->ny < 16 || p->nx > 4096 || p->ny > 4096)
+    return fail(HOS_ERR_ARG, "grid %dx%d: sizes must be powers of two in [16, 4096]", p->nx, p->ny);
+  if (p->order < 1 || p->order > 7) return fail(HOS_ERR_ARG, "order M=%d outside 1..7", p->order);
+  if (p->precision != HOS_PREC_FP64 && p->precision != HOS_PREC_FP32)
+    return fail(HOS_ERR_ARG, "precision %d", p->precision);
+  if (!(p->lx > 0) || !(p->ly > 0)) return fail(HOS_ERR_ARG, "domain lengths must be positive");
+  if (p->rampflg == 1 && !(p->tramp != 0)) return fail(HOS_ERR_ARG, "ramp with Tramp = 0");
+  hos_ctx* c = new hos_ctx();
+  c->p = *p;
+  c->nx = p->nx;
+  c->ny = p->ny;
+  c->h = p->ny / 2;
+  c->M = p->order;
+  c->L = p->order - 1;
+  c->prec = p->precision;
+  if (butcher(p->scheme, &c->nst, c->b, c->c)) {
+    delete c;
+    return fail(HOS_ERR_ARG, "unknown scheme %d", p->scheme);
+  }
+  cudaGetDevice(&c->device);
+  Geo& G = c->geo;
+  G.nx = c->nx;
+  G.ny = c->ny;
+  G.h = c->h;
+  // operators_par.c:290-291
+  G.mx = p->mx > 0 ? p->mx : (int)std::floor(0.5 * c->nx / (1 + 0.5 * c->L));
+  G.my = p->my > 0 ? p->my : (int)std::floor(0.5 * c->ny / (1 + 0.5 * c->L));
+  if (G.my > c->h + 1) G.my = c->h + 1;
+  if (G.my < 1) G.my = 1;
+  G.kx0 = 2 * M_PI / p->lx;  // hdf5_routines_2d_par.c:98-99
+  G.ky0 = 2 * M_PI / p->ly;
+  G.depth = p->depth;
+  G.g = p->g;
+  G.inv_nxny = 1.0 / ((double)c->nx * (double)c->ny);
+  c->fsz = (size_t)(c->h + 1) * c->nx;
+  c->psz = (size_t)c->nx * c->ny;
+  c->nz = 4 + c->M;
+  c->nphys = 5 + c->M * (c->M + 1) / 2 + c->L;
+  const size_t cs = c->prec ? sizeof(float2) : sizeof(double2);
+  const size_t rs = c->prec ? sizeof(float) : sizeof(double);
+  int rc = HOS_OK;
+  cudaError_t e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete c;
+    return fail(HOS_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+  }
+#define HOS_AL(ptr, bytes)          \
+  do {                              \
+    rc = dalloc(&(ptr), (bytes));   \
+    if (rc) {                       \
+      release(c);                   \
+      return rc;                    \
+    }                               \
+  } while (0)
+  HOS_AL(c->u, 2 * c->fsz * sizeof(double2));
+  HOS_AL(c->k, (size_t)c->nst * 2 * c->fsz * sizeof(double2));
+  HOS_AL(c->zbuf, (size_t)c->nz * c->fsz * cs);
+  HOS_AL(c->phys, (size_t)c->nphys * c->psz * rs);
+  HOS_AL(c->ustage, 2 * c->fsz * sizeof(double2));
+  HOS_AL(c->zplain, c->fsz * sizeof(double2));
+  HOS_AL(c->pplain, 2 * c->psz * sizeof(double));
+  HOS_AL(c->tw64, TW_N * sizeof(double2));
+  HOS_AL(c->tw32, TW_N * sizeof(float2));
+  HOS_AL(c->tdev, sizeof(double));
+  HOS_AL(c->trhs, sizeof(double));
+  HOS_AL(c->rdev, sizeof(double));
+  HOS_AL(c->stepdev, sizeof(long long));
+  HOS_AL(c->actdev, sizeof(int));
+  HOS_AL(c->flagdev, sizeof(int));
+  HOS_AL(c->ham_hist, HIST_CAP * sizeof(double));
+  HOS_AL(c->t_hist, HIST_CAP * sizeof(double));
+#undef HOS_AL
+  rc = make_cfg(c, c->prec, &c->cfg);
+  if (!rc) rc = make_cfg(c, 0, &c->cfg64);
+  if (rc) {
+    release(c);
+    return rc;
+  }
+  c->nparts = xgrid(c, c->cfg);
+  rc = dalloc(&c->ham_part, (size_t)c->nparts * sizeof(double));
+  if (rc) {
+    release(c);
+    return rc;
+  }
+  // twiddles, zeroed state and stage buffers (rows ky >= my of k are never written)
+  std::vector<double2> tw = twiddle_table();
+  std::vector<float2> tw32(TW_N);
+  for (int i = 0; i < TW_N; i++) tw32[i] = make_float2((float)tw[i].x, (float)tw[i].y);
+  e = cudaMemcpy(c->tw64, tw.data(), TW_N * sizeof(double2), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(c->tw32, tw32.data(), TW_N * sizeof(float2), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->u, 0, 2 * c->fsz * sizeof(double2), c->st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->k, 0, (size_t)c->nst * 2 * c->fsz * sizeof(double2), c->st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->tdev, 0, sizeof(double), c->st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->stepdev, 0, sizeof(long long), c->st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->ham_part, 0, (size_t)c->nparts * sizeof(double), c->st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->ham_hist, 0, HIST_CAP * sizeof(double), c->st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->t_hist, 0, HIST_CAP * sizeof(double), c->st);
+  if (e == cudaSuccess) {
+    k_set_int<<<1, 32, 0, c->st>>>(c->actdev, c->geo.my);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+  if (e != cudaSuccess) {
+    release(c);
+    return fail(HOS_ERR_CUDA, "init: %s", cudaGetErrorString(e));
+  }
+  *out = c;
+  return HOS_OK;
+}
+
+int hos_destroy(hos_handle h) {
+  if (!h) return HOS_OK;
+  cudaStreamSynchronize(h->st);
+  release(h);
+  return HOS_OK;
+}
+
+int hos_get_bounds(hos_handle h, int* mx, int* my) {
+  if (!h) return fail(HOS_ERR_ARG, "null handle");
+  if (mx) *mx = h->geo.mx;
+  if (my) *my = h->geo.my;
+  return HOS_OK;
+}
+
+void* hos_stream(hos_handle h) { return h ? (void*)h->st : nullptr; }
+
+int hos_set_state_spectral(hos_handle h, const double* u, double t) {
+  if (!h || !u) return fail(HOS_ERR_ARG, "null argument");
+  HOS_CK(cudaMemcpyAsync(h->u, u, 2 * h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+  HOS_CK(cudaMemcpyAsync(h->tdev, &t, sizeof(double), cudaMemcpyHostToDevice, h->st));
+  refresh_active_rows(h, h->u, h->actdev);
+  HOS_CK(cudaGetLastError());
+  HOS_CK(cudaStreamSynchronize(h->st));
+  return HOS_OK;
+}
+
+int hos_get_state_spectral(hos_handle h, double* u, double* t) {
+  if (!h || !u) return fail(HOS_ERR_ARG, "null argument");
+  HOS_CK(cudaMemcpyAsync(u, h->u, 2 * h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+  double tt = 0;
+  HOS_CK(cudaMemcpyAsync(&tt, h->tdev, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  HOS_CK(cudaStreamSynchronize(h->st));
+  if (t) *t = tt;
+  return HOS_OK;
+}
+
+int hos_set_state_physical(hos_handle h, const double* eta, const double* phi, double t) {
+  if (!h || !eta || !phi) return fail(HOS_ERR_ARG, "null argument");
+  HOS_CK(cudaMemcpyAsync(h->pplain, eta, h->psz * sizeof(double), cudaMemcpyDefault, h->st));
+  HOS_CK(cudaMemcpyAsync(h->pplain + h->psz, phi, h->psz * sizeof(double), cudaMemcpyDefault, h->st));
+  enqueue_r2c(h, h->pplain, h->u, 1);
+  enqueue_r2c(h, h->pplain + h->psz, h->u + h->fsz, 1);
+  HOS_CK(cudaMemcpyAsync(h->tdev, &t, sizeof(double), cudaMemcpyHostToDevice, h->st));
+  refresh_active_rows(h, h->u, h->actdev);
+  HOS_CK(cudaGetLastError());
+  HOS_CK(cudaStreamSynchronize(h->st));
+  return HOS_OK;
+}
+
+int hos_get_state_physical(hos_handle h, double* eta, double* phi) {
+  if (!h || !eta || !phi) return fail(HOS_ERR_ARG, "null argument");
+  enqueue_c2r(h, h->u, h->pplain);
+  enqueue_c2r(h, h->u + h->fsz, h->pplain + h->psz);
+  HOS_CK(cudaGetLastError());
+  HOS_CK(cudaMemcpyAsync(eta, h->pplain, h->psz * sizeof(double), cudaMemcpyDefault, h->st));
+  HOS_CK(cudaMemcpyAsync(phi, h->pplain + h->psz, h->psz * sizeof(double), cudaMemcpyDefault, h->st));
+  HOS_CK(cudaStreamSynchronize(h->st));
+  return HOS_OK;
+}
+
+int hos_step(hos_handle h, double dt, int nsteps) {
+  if (!h) return fail(HOS_ERR_ARG, "null handle");
+  if (nsteps < 0) return fail(HOS_ERR_ARG, "nsteps < 0");
+  if (nsteps == 0) return HOS_OK;
+  int rc = build_graph(h, dt);
+  if (rc) return rc;
+  for (int i = 0; i < nsteps; i++) HOS_CK(cudaGraphLaunch(h->gexec, h->st));
+  return HOS_OK;
+}
+
+int hos_sync(hos_handle h) {
+  if (!h) return fail(HOS_ERR_ARG, "null handle");
+  HOS_CK(cudaStreamSynchronize(h->st));
+  HOS_CK(cudaGetLastError());
+  return HOS_OK;
+}
+
+int hos_energy_history(hos_handle h, double* t_out, double* ham_out, int max, int* count) {
+  if (!h || !count) return fail(HOS_ERR_ARG, "null argument");
+  long long steps = 0;
+  HOS_CK(cudaMemcpyAsync(&steps, h->stepdev, sizeof(long long), cudaMemcpyDeviceToHost, h->st));
+  HOS_CK(cudaStreamSynchronize(h->st));
+  long long first = h->hist_base;
+  if (steps - first > HIST_CAP) first = steps - HIST_CAP;
+  long long n = steps - first;
+  if (n > max) {
+    first = steps - max;
+    n = max;
+  }
+  std::vector<double> th(HIST_CAP), hh(HIST_CAP);
+  if (n > 0) {
+    HOS_CK(cudaMemcpy(th.data(), h->t_hist, HIST_CAP * sizeof(double), cudaMemcpyDeviceToHost));
+    HOS_CK(cudaMemcpy(hh.data(), h->ham_hist, HIST_CAP * sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  for (long long i = 0; i < n; i++) {
+    const long long s = first + i;
+    const size_t slot = (size_t)(s % HIST_CAP);
+    if (t_out) t_out[i] = th[slot];
+    if (ham_out) ham_out[i] = hh[slot];
+  }
+  *count = (int)n;
+  return HOS_OK;
+}
+
+int hos_clear_history(hos_handle h) {
+  if (!h) return fail(HOS_ERR_ARG, "null handle");
+  long long steps = 0;
+  HOS_CK(cudaMemcpyAsync(&steps, h->stepdev, sizeof(long long), cudaMemcpyDeviceToHost, h->st));
+  HOS_CK(cudaStreamSynchronize(h->st));
+  h->hist_base = steps;
+  return HOS_OK;
+}
+
+int hos_rhs(hos_handle h, const double* u, double* rhs, double t) {
+  if (!h || !u || !rhs) return fail(HOS_ERR_ARG, "null argument");
+  HOS_CK(cudaMemcpyAsync(h->ustage, u, 2 * h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+  HOS_CK(cudaMemcpyAsync(h->trhs, &t, sizeof(double), cudaMemcpyHostToDevice, h->st));
+  // the last stage buffer is scratch between steps; rows ky >= my stay zero
+  double2* kout = h->k + (size_t)(h->nst - 1) * 2 * h->fsz;
+  int rc = enqueue_stage(h, 0, 0.0, true, h->ustage, kout, h->trhs, nullptr);
+  if (rc) return rc;
+  HOS_CK(cudaGetLastError());
+  HOS_CK(cudaMemcpyAsync(rhs, kout, 2 * h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+  HOS_CK(cudaStreamSynchronize(h->st));
+  return HOS_OK;
+}
+
+int hos_fft_2d(hos_handle h, const double* u_phys, double* hu) {
+  if (!h || !u_phys || !hu) return fail(HOS_ERR_ARG, "null argument");
+  HOS_CK(cudaMemcpyAsync(h->pplain, u_phys, h->psz * sizeof(double), cudaMemcpyDefault, h->st));
+  enqueue_r2c(h, h->pplain, h->ustage, 0);
+  HOS_CK(cudaGetLastError());
+  HOS_CK(cudaMemcpyAsync(hu, h->ustage, h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+  HOS_CK(cudaStreamSynchronize(h->st));
+  return HOS_OK;
+}
+
+int hos_ifft_2d(hos_handle h, const double* hu, double* u_phys) {
+  if (!h || !hu || !u_phys) return fail(HOS_ERR_ARG, "null argument");
+  HOS_CK(cudaMemcpyAsync(h->ustage, hu, h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+  enqueue_c2r(h, h->ustage, h->pplain);
+  HOS_CK(cudaGetLastError());
+  HOS_CK(cudaMemcpyAsync(u_phys, h->pplain, h->psz * sizeof(double), cudaMemcpyDefault, h->st));
+  HOS_CK(cudaStreamSynchronize(h->st));
+  return HOS_OK;
+}
+
+int hos_check_finite(hos_handle h, int* finite) {
+  if (!h || !finite) return fail(HOS_ERR_ARG, "null argument");
+  HOS_CK(cudaMemsetAsync(h->flagdev, 0, sizeof(int), h->st));
+  k_nonfinite<<<148, 256, 0, h->st>>>(h->u, 2 * h->fsz, h->flagdev);
+  int f = 0;
+  HOS_CK(cudaGetLastError());
+  HOS_CK(cudaMemcpyAsync(&f, h->flagdev, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  HOS_CK(cudaStreamSynchronize(h->st));
+  *finite = f ? 0 : 1;
+  return HOS_OK;
+}
+
+int hos_volume(hos_handle h, double* vol) {
+  if (!h || !vol) return fail(HOS_ERR_ARG, "null argument");
+  double2 v;
+  HOS_CK(cudaMemcpyAsync(&v, h->u, sizeof(double2), cudaMemcpyDeviceToHost, h->st));
+  HOS_CK(cudaStreamSynchronize(h->st));
+  *vol = v.x;
+  return HOS_OK;
+}
+
+}  // extern "C"

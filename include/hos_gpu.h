@@ -1,0 +1,138 @@
+/*
+ * hos_gpu.h -- C ABI of the B200 (sm_100a) HOS time-advance library
+ * (libhos_gpu.so).
+ *
+ * Two groups of entry points live in the library.
+ *
+ * 1. Handle API (this header).  A handle owns one wave field (or one ensemble
+ *    member): its FP64 spectral state resident in GPU memory, its scratch,
+ *    its CUDA stream and its captured step graph.  Every call returns an int
+ *    status (HOS_OK or an HOS_ERR_* code); hos_last_error() describes the
+ *    most recent failure of the calling thread.  Calls on one handle must not
+ *    overlap; different handles may be driven from different threads.
+ *
+ * 2. Reference-compatible symbols (hos_legacy.h): the functions of the
+ *    reference's Csource/2dpar hot path with their original signatures, so
+ *    that the unchanged host driver main_2d_par.c links against this library
+ *    in place of time_schemes_par.o, hosm_2d_par.o, operators_par.o and
+ *    fft_routines_2d_par.o.
+ *
+ * Array conventions (host or device, always double precision at the ABI):
+ *   physical field : real [nx][ny], row-major (x major, y contiguous), unpadded;
+ *   spectral field : complex [ny/2+1][nx] as interleaved (re, im) doubles --
+ *                    the reference's single-rank FFTW_MPI_TRANSPOSED_OUT
+ *                    layout (main_2d_par.c:189, Dx at operators_par.c:66);
+ *   packed state   : [eta_hat | phi_hat], two spectral fields back to back
+ *                    (main_2d_par.c:150,158; sol_update_RK's u).
+ * Spectral fields are normalised by 1/(nx*ny) as fft_2d does
+ * (fft_routines_2d_par.c:53-55).
+ */
+#ifndef HOS_GPU_H
+#define HOS_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  HOS_OK = 0,
+  HOS_ERR_ARG = 1,       /* invalid argument (size, order, scheme, null pointer) */
+  HOS_ERR_CUDA = 2,      /* a CUDA call failed */
+  HOS_ERR_NOMEM = 3,     /* device memory exhausted */
+  HOS_ERR_NONFINITE = 4, /* the state contains NaN or Inf */
+  HOS_ERR_STATE = 5,     /* call not valid in the handle's current state */
+  HOS_ERR_TIMEOUT = 6,   /* a bounded wait ran out */
+  HOS_ERR_BUSY = 7       /* admission refused (no slot or memory) */
+};
+
+enum { HOS_PREC_FP64 = 0, HOS_PREC_FP32 = 1 };
+
+/* Runge-Kutta scheme ids of Setup_TimeScheme (time_schemes_par.c:127-314). */
+enum { HOS_RK45DP = 1, HOS_RK4 = 2, HOS_EULER = 3, HOS_MIDPOINT = 4, HOS_HEUN = 5 };
+
+typedef struct hos_params {
+  int nx, ny;       /* grid, powers of two, 16 <= nx <= 4096, 16 <= ny <= 4096 */
+  double lx, ly;    /* domain lengths (Kx0 = 2 pi / Lx, hdf5_routines_2d_par.c:98-99) */
+  double g;         /* gravity */
+  int order;        /* HOS order M = NLevs + 1 (euler_2d_par.h:24), 1..7 */
+  int precision;    /* HOS_PREC_FP64 (drop-in) or HOS_PREC_FP32 (FP32 transforms, FP64 state) */
+  double depth;     /* <= 0: deep water (the reference); > 0: finite depth h */
+  int rampflg;      /* Dommermuth ramp on/off (hosm_2d_par.c:211-229) */
+  double tramp;     /* ramp time scale Tramp */
+  int scheme;       /* HOS_RK4 etc. */
+  int mx, my;       /* dealias bounds; 0 selects the reference rule (operators_par.c:290-291) */
+} hos_params;
+
+typedef struct hos_ctx* hos_handle;
+
+/* Fills p with the reference defaults for an nx x ny grid (M = 3, RK4,
+ * FP64, deep water, no ramp, 2 pi x 2 pi, g = 1). */
+void hos_default_params(hos_params* p, int nx, int ny);
+
+/* Creates a handle on the current CUDA device and a stream of its own.
+ * Replaces the allocations of rhs_hos_setup (hosm_2d_par.c:51-97) and
+ * Setup_TimeScheme (time_schemes_par.c:127-196). */
+int hos_create(const hos_params* p, hos_handle* out);
+int hos_destroy(hos_handle h);
+
+/* Device bytes a handle with these parameters allocates (admission control). */
+size_t hos_footprint_bytes(const hos_params* p);
+
+/* Dealias bounds in effect (mx, my) for a handle. */
+int hos_get_bounds(hos_handle h, int* mx, int* my);
+
+/* State transfer.  *_spectral take/return the packed state (2*(ny/2+1)*nx
+ * complex).  set_state_physical applies fft_2d and Dealias to eta and phi
+ * exactly as main_2d_par.c:258-262; get_state_physical applies ifft_2d as
+ * main_2d_par.c:310-311.  Pointers may be host (pageable or pinned) or
+ * device memory. */
+int hos_set_state_spectral(hos_handle h, const double* u, double t);
+int hos_get_state_spectral(hos_handle h, double* u, double* t);
+int hos_set_state_physical(hos_handle h, const double* eta, const double* phi, double t);
+int hos_get_state_physical(hos_handle h, double* eta, double* phi);
+
+/* Advances nsteps RK steps of size dt on the device (sol_update_RK,
+ * time_schemes_par.c:28-121, called nsteps times).  Asynchronous with
+ * respect to the host; hos_sync waits. */
+int hos_step(hos_handle h, double dt, int nsteps);
+int hos_sync(hos_handle h);
+
+/* Stage-0 Hamiltonian of each step (hosm_2d_par.c:462-523, logged by the
+ * reference to runtime.dat at time_schemes_par.c:73-93) and the step-start
+ * time it belongs to, oldest first.  Returns the number of records written
+ * in *count (at most max).  hos_clear_history empties the record. */
+int hos_energy_history(hos_handle h, double* t_out, double* ham_out, int max, int* count);
+int hos_clear_history(hos_handle h);
+
+/* One right-hand-side evaluation rhs_hos(rhs, u, t) (hosm_2d_par.c:138-235)
+ * on a packed spectral state; does not touch the handle's state. */
+int hos_rhs(hos_handle h, const double* u, double* rhs, double t);
+
+/* fft_2d / ifft_2d (fft_routines_2d_par.c:21-103) on the handle's grid:
+ * normalised r2c of a physical field and unnormalised c2r of a spectral one. */
+int hos_fft_2d(hos_handle h, const double* u_phys, double* hu);
+int hos_ifft_2d(hos_handle h, const double* hu, double* u_phys);
+
+/* Whether the resident state is finite (1) or holds NaN/Inf (0). */
+int hos_check_finite(hos_handle h, int* finite);
+
+/* Volume (the k = 0 mode of eta_hat, real part) of the resident state. */
+int hos_volume(hos_handle h, double* vol);
+
+/* CUDA stream of the handle (a cudaStream_t), for callers that order their
+ * own work against it. */
+void* hos_stream(hos_handle h);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* hos_last_error(void);
+
+/* Library build description (kernel set, architecture). */
+const char* hos_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HOS_GPU_H */

@@ -1,0 +1,210 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle.
+
+FP64 drop-in: results must match the reference CPU path to 1e-10 relative
+after 100 RK4 steps; single operator evaluations to 1e-12.  The FP32-compute
+form is held to the error it documents (relative to the FP64 result)."""
+import math
+
+import numpy as np
+import pytest
+
+from hos_b200 import HosField, ic
+from oracle.hos_np import HosNumpy
+
+pytestmark = pytest.mark.gpu
+
+TOL_OP = 1e-12     # one RHS / transform, FP64
+TOL_STEPS = 1e-10  # after up to 100 RK steps, FP64 (the drop-in gate)
+
+
+def rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def test_fft_pair_matches_golden(golden):
+    d = golden("fft_32x16")
+    with HosField(32, 16) as f:
+        assert rel(f.fft_2d(d["x"]), d["hx"]) < 1e-14
+        assert rel(f.ifft_2d(d["s"]), d["xs"]) < 1e-14
+
+
+@pytest.mark.parametrize("nx,ny", [(16, 16), (64, 128), (256, 32), (1024, 1024), (2048, 512), (4096, 64)])
+def test_fft_pair_random(nx, ny):
+    rng = np.random.default_rng(nx + ny)
+    hn = HosNumpy(nx, ny, 2 * math.pi, 2 * math.pi, 1.0, 3)
+    x = rng.standard_normal((nx, ny))
+    s = rng.standard_normal((ny // 2 + 1, nx)) + 1j * rng.standard_normal((ny // 2 + 1, nx))
+    with HosField(nx, ny) as f:
+        assert rel(f.fft_2d(x), hn.fft2(x)) < 1e-13
+        assert rel(f.ifft_2d(s), hn.ifft2(s)) < 1e-13
+
+
+@pytest.mark.parametrize("name", ["rhs_m4_32x16_d_r1", "rhs_m3_32x32_nd_r0", "rhs_m5_64x64_d_r1",
+                                  "rhs_m6_32x64_d_r0", "rhs_m1_16x16_nd_r0", "rhs_m2_16x32_d_r1"])
+def test_rhs_matches_golden(golden, name):
+    d = golden(name)
+    nx, ny, M, ramp = (int(v) for v in d["meta"])
+    with HosField(nx, ny, order=M, g=float(d["g"]), rampflg=ramp, tramp=float(d["tramp"])) as f:
+        r = f.rhs(d["u"], float(d["t"]))
+    assert rel(r[0], d["rhs"][0]) < TOL_OP
+    assert rel(r[1], d["rhs"][1]) < TOL_OP
+
+
+def test_init_state_matches_golden(golden):
+    d = golden("stokes64_m3_rk4_100")
+    with HosField(64, 64, order=3) as f:
+        f.set_state_physical(d["eta0"], d["phi0"])
+        u, t = f.state_spectral()
+    assert rel(u, d["u0"]) < 1e-14 and t == 0.0
+
+
+def test_stokes_100_rk4_steps_drop_in_gate(golden):
+    """First configuration: 64^2, M=3, Stokes ka=0.1, RK4 dt=T/64, 100 steps."""
+    d = golden("stokes64_m3_rk4_100")
+    hn = HosNumpy(64, 64, 2 * math.pi, 2 * math.pi, 1.0, 3)
+    with HosField(64, 64, order=3) as f:
+        f.set_state_physical(d["eta0"], d["phi0"])
+        f.step(float(d["dt"]), 100)
+        u, t = f.state_spectral()
+        tt, H = f.energy_history()
+        eta, phi = f.state_physical()
+    assert rel(u[0], d["u100"][0]) < TOL_STEPS
+    assert rel(u[1], d["u100"][1]) < TOL_STEPS
+    # physical eta, phi_s as the survey's parity metric states it
+    assert rel(eta, hn.ifft2(d["u100"][0])) < TOL_STEPS
+    assert rel(phi, hn.ifft2(d["u100"][1])) < TOL_STEPS
+    assert abs(t - float(d["t100"])) < 1e-12
+    assert len(H) == 100
+    assert np.max(np.abs(H - d["ham"])) / np.max(np.abs(d["ham"])) < TOL_STEPS
+    assert abs(tt[0]) < 1e-15 and abs(tt[-1] - 99 * float(d["dt"])) < 1e-9
+
+
+@pytest.mark.parametrize("scheme", [1, 2, 3, 4, 5])
+def test_schemes_match_golden(golden, scheme):
+    d = golden(f"scheme{scheme}_32_m4")
+    with HosField(32, 32, order=4, scheme=scheme) as f:
+        f.set_state_spectral(d["u0"], 0.0)
+        f.step(float(d["dt"]), 5)
+        u, t = f.state_spectral()
+        _, H = f.energy_history()
+    assert rel(u, d["u5"]) < TOL_STEPS
+    assert np.max(np.abs(H - d["ham"])) / np.max(np.abs(d["ham"])) < TOL_STEPS
+
+
+def test_jonswap_ramp_m5_matches_golden(golden):
+    d = golden("jonswap64_m5_ramp_20")
+    L = float(d["lx"])
+    with HosField(64, 64, order=5, lx=L, ly=L, g=9.81, rampflg=1, tramp=200.0) as f:
+        f.set_state_physical(d["eta0"], d["phi0"])
+        f.step(0.2, 20)
+        u, t = f.state_spectral()
+        _, H = f.energy_history()
+    assert rel(u, d["u20"]) < TOL_STEPS
+    assert np.max(np.abs(H - d["ham"])) / np.max(np.abs(d["ham"])) < TOL_STEPS
+
+
+@pytest.mark.parametrize("M,nx,ny", [(4, 512, 512), (5, 256, 128), (3, 128, 256), (6, 64, 64), (7, 32, 32)])
+def test_rhs_random_sizes_vs_restatement(M, nx, ny):
+    rng = np.random.default_rng(M * 1000 + nx)
+    hn = HosNumpy(nx, ny, 2 * math.pi, 2 * math.pi, 1.0, M)
+    u = 1e-3 * (rng.standard_normal((2, ny // 2 + 1, nx)) + 1j * rng.standard_normal((2, ny // 2 + 1, nx)))
+    u[0] = hn.Dealias(u[0])
+    u[1] = hn.Dealias(u[1])
+    with HosField(nx, ny, order=M) as f:
+        r = f.rhs(u, 0.0)
+    re_, rp = hn.rhs(u[0], u[1], 0.0)
+    assert rel(r[0], re_) < TOL_OP
+    assert rel(r[1], rp) < TOL_OP
+
+
+def test_non_dealiased_state_steps_vs_restatement():
+    """A state with content beyond the dealias bounds exercises the kx quirk
+    and the c2r projection on every pass."""
+    rng = np.random.default_rng(5)
+    nx, ny, M = 32, 32, 3
+    hn = HosNumpy(nx, ny, 2 * math.pi, 2 * math.pi, 1.0, M)
+    u = 1e-3 * (rng.standard_normal((2, 17, 32)) + 1j * rng.standard_normal((2, 17, 32)))
+    e, p, t = u[0].copy(), u[1].copy(), 0.0
+    for _ in range(3):
+        e, p, t, _h = hn.step(e, p, t, 0.05, 2)
+    with HosField(nx, ny, order=M) as f:
+        f.set_state_spectral(u, 0.0)
+        f.step(0.05, 3)
+        g, _ = f.state_spectral()
+    assert rel(g[0], e) < TOL_STEPS and rel(g[1], p) < TOL_STEPS
+
+
+def test_finite_depth_rhs_vs_restatement():
+    rng = np.random.default_rng(8)
+    nx = ny = 64
+    for M in (3, 5):
+        hn = HosNumpy(nx, ny, 2 * math.pi, 2 * math.pi, 1.0, M, depth=0.3)
+        u = 1e-3 * (rng.standard_normal((2, 33, 64)) + 1j * rng.standard_normal((2, 33, 64)))
+        u[0], u[1] = hn.Dealias(u[0]), hn.Dealias(u[1])
+        with HosField(nx, ny, order=M, depth=0.3) as f:
+            r = f.rhs(u, 0.0)
+        re_, rp = hn.rhs(u[0], u[1], 0.0)
+        assert rel(r[0], re_) < TOL_OP and rel(r[1], rp) < TOL_OP
+
+
+def test_dealias_override_vs_restatement():
+    rng = np.random.default_rng(9)
+    nx = ny = 64
+    hn = HosNumpy(nx, ny, 2 * math.pi, 2 * math.pi, 1.0, 4, mx=21, my=21)
+    u = 1e-3 * (rng.standard_normal((2, 33, 64)) + 1j * rng.standard_normal((2, 33, 64)))
+    u[0], u[1] = hn.Dealias(u[0]), hn.Dealias(u[1])
+    with HosField(nx, ny, order=4, mx=21, my=21) as f:
+        assert f.bounds == (21, 21)
+        r = f.rhs(u, 0.0)
+    re_, rp = hn.rhs(u[0], u[1], 0.0)
+    assert rel(r[0], re_) < TOL_OP and rel(r[1], rp) < TOL_OP
+
+
+def test_fp32_form_error_is_small():
+    """FP32 transforms/products with FP64 state: 200 RK4 steps of a JONSWAP
+    sea stay within 1e-5 Hs of the FP64 run."""
+    nx = ny = 128
+    eta, phi, info = ic.jonswap(nx, ny, kp=12.0, steepness=0.1, seed=3)
+    dt = info["Tp"] / 50
+    out = {}
+    for prec in ("fp64", "fp32"):
+        with HosField(nx, ny, order=5, precision=prec) as f:
+            f.set_state_physical(eta, phi)
+            f.step(dt, 200)
+            out[prec] = f.state_physical()
+    err = np.max(np.abs(out["fp32"][0] - out["fp64"][0]))
+    assert err < 1e-5 * info["Hs"], err
+
+
+def test_deterministic_and_volume_conserved():
+    eta, phi, info = ic.jonswap(64, 64, kp=8.0, steepness=0.1, seed=4)
+    res = []
+    for _ in range(2):
+        with HosField(64, 64, order=4) as f:
+            f.set_state_physical(eta, phi)
+            v0 = f.volume()
+            f.step(info["Tp"] / 50, 30)
+            u, _ = f.state_spectral()
+            assert abs(f.volume() - v0) < 1e-15
+            assert f.is_finite()
+            res.append(u)
+    assert np.array_equal(res[0], res[1])
+
+
+def test_nonfinite_state_is_reported():
+    with HosField(32, 32) as f:
+        u = np.zeros((2, 17, 32), complex)
+        u[0, 0, 1] = np.nan
+        f.set_state_spectral(u)
+        assert not f.is_finite()
+
+
+def test_bad_arguments_raise():
+    from hos_b200 import HosError
+
+    with pytest.raises(HosError):
+        HosField(48, 64)
+    with pytest.raises(HosError):
+        HosField(64, 64, order=9)
+    with pytest.raises(HosError):
+        HosField(64, 64, scheme=7)
