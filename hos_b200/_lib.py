@@ -47,6 +47,15 @@ class HosParams(ctypes.Structure):
     ]
 
 
+class HosPassStat(ctypes.Structure):
+    _fields_ = [
+        ("name", ctypes.c_char * 32),
+        ("launches_per_stage", ctypes.c_int),
+        ("ms_per_launch", ctypes.c_double),
+        ("bytes_per_launch", ctypes.c_double),
+    ]
+
+
 class HosError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"hos error {code}: {msg}")
@@ -82,6 +91,8 @@ _SIGNATURES = {
     "hos_check_finite": (_I, [_H, ctypes.POINTER(_I)]),
     "hos_volume": (_I, [_H, _DP]),
     "hos_stream": (_P, [_H]),
+    "hos_profile_stage": (_I, [_H, _D, _I, ctypes.POINTER(HosPassStat), _I, ctypes.POINTER(_I)]),
+    "hos_launches_per_step": (_I, [_H]),
     "hos_last_error": (ctypes.c_char_p, []),
     "hos_version": (ctypes.c_char_p, []),
 }

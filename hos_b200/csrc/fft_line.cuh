@@ -15,8 +15,8 @@
 // R-point DFT and writes y[(j/Ns)*Ns*R + j mod Ns + r*Ns].  N = E^s * R' with
 // a final pass of radix R' < E in which each thread runs E/R' butterflies.
 //
-// Twiddles come from a host-computed table of exp(-2 pi i k / TW_N) (long
-// double libm on the host, rounded once).
+// Twiddles come from a host-computed table of exp(-2 pi i k / N) for the
+// line length N (long double libm on the host, rounded once).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -24,7 +24,6 @@
 
 namespace hos {
 
-constexpr int TW_N = 8192;  // master twiddle table length (max line length)
 
 template <typename T>
 struct CpxOf;
@@ -208,7 +207,7 @@ __host__ __device__ constexpr int line_smem_elems() {
   return N + N / E;
 }
 
-// Twiddle exp(sgn 2 pi i a / n) from the master table.
+// Twiddle exp(-+2 pi i a*scale / N) from the length-N table.
 template <bool INV, typename C>
 __device__ __forceinline__ C twid(const C* __restrict__ tw, int a, int scale) {
   C w = __ldg(&tw[a * scale]);
@@ -227,7 +226,7 @@ struct LinePlan {
 
 // Runs the line FFT in place on v.  All threads of the block must call it
 // (it contains __syncthreads); sm is this line's padded buffer of
-// line_smem_elems<N,E>() elements.
+// line_smem_elems<N,E>() elements; tw is the length-N twiddle table.
 template <typename T, int N, int E, bool INV>
 __device__ __forceinline__ void line_fft(cpx<T> (&v)[E], cpx<T>* sm, int t, const cpx<T>* __restrict__ tw) {
   using C = cpx<T>;
@@ -240,7 +239,7 @@ __device__ __forceinline__ void line_fft(cpx<T> (&v)[E], cpx<T>* sm, int t, cons
   for (int s = 0; s < SF; s++) {
     if (s > 0) {
       const int jm = t & (ns - 1);
-      const int scale = TW_N / (ns * E);
+      const int scale = N / (ns * E);
 #pragma unroll
       for (int r = 1; r < E; r++) v[r] = cmul(v[r], twid<INV>(tw, r * jm, scale));
     }
@@ -259,7 +258,7 @@ __device__ __forceinline__ void line_fft(cpx<T> (&v)[E], cpx<T>* sm, int t, cons
   }
   if (RL > 1) {
     constexpr int Q = E / RL;
-    const int scale = TW_N / N;
+    const int scale = 1;
 #pragma unroll
     for (int q = 0; q < Q; q++) {
       C a[RL > 1 ? RL : 1];

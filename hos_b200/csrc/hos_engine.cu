@@ -28,18 +28,18 @@
 #include "hos_registry.h"
 
 namespace hos {
-XInvFn lookup_xinv_64(int n);
-XFwdFn lookup_xfwd_64(int n);
-YInvFn lookup_yinv_64(int h);
-YFwdFn lookup_yfwd_64(int h);
-XInvFn lookup_xinv_32(int n);
-XFwdFn lookup_xfwd_32(int n);
-YInvFn lookup_yinv_32(int h);
-YFwdFn lookup_yfwd_32(int h);
-XInvFn lookup_xinv(int prec, int n) { return prec ? lookup_xinv_32(n) : lookup_xinv_64(n); }
-XFwdFn lookup_xfwd(int prec, int n) { return prec ? lookup_xfwd_32(n) : lookup_xfwd_64(n); }
-YInvFn lookup_yinv(int prec, int h) { return prec ? lookup_yinv_32(h) : lookup_yinv_64(h); }
-YFwdFn lookup_yfwd(int prec, int h) { return prec ? lookup_yfwd_32(h) : lookup_yfwd_64(h); }
+XInvFn lookup_xinv_64(int mode, int n);
+XFwdFn lookup_xfwd_64(int mode, int n);
+YInvFn lookup_yinv_64(int mode, int h);
+YFwdFn lookup_yfwd_64(int mode, int h);
+XInvFn lookup_xinv_32(int mode, int n);
+XFwdFn lookup_xfwd_32(int mode, int n);
+YInvFn lookup_yinv_32(int mode, int h);
+YFwdFn lookup_yfwd_32(int mode, int h);
+XInvFn lookup_xinv(int prec, int mode, int n) { return prec ? lookup_xinv_32(mode, n) : lookup_xinv_64(mode, n); }
+XFwdFn lookup_xfwd(int prec, int mode, int n) { return prec ? lookup_xfwd_32(mode, n) : lookup_xfwd_64(mode, n); }
+YInvFn lookup_yinv(int prec, int mode, int h) { return prec ? lookup_yinv_32(mode, h) : lookup_yinv_64(mode, h); }
+YFwdFn lookup_yfwd(int prec, int mode, int h) { return prec ? lookup_yfwd_32(mode, h) : lookup_yfwd_64(mode, h); }
 
 // ---------------------------------------------------------------- small kernels
 __global__ void k_set_int(int* p, int v) {
@@ -71,16 +71,24 @@ __global__ void k_nonfinite(const double2* u, size_t n, int* flag) {
 }
 
 // ---------------------------------------------------------------- step end
-// Sums the stage-0 Hamiltonian partials in a fixed order, records (t, H) and
-// advances t (time_schemes_par.c:73-93,119).
-__global__ void k_step_end(const double* ham_part, int nparts, double* tdev, double dt, long long* stepdev,
-                           double* ham_hist, double* t_hist, int hist_cap) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// Sums the stage-0 Hamiltonian partials in a fixed order (one block, fixed
+// strides, fixed tree), records (t, H) and advances t
+// (time_schemes_par.c:73-93,119).
+__global__ void __launch_bounds__(256) k_step_end(const double* ham_part, int nparts, double* tdev, double dt,
+                                                  long long* stepdev, double* ham_hist, double* t_hist, int hist_cap) {
+  __shared__ double red[256];
   double s = 0.0;
-  for (int i = 0; i < nparts; i++) s += ham_part[i];
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) s += ham_part[i];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
   const long long st = *stepdev;
   if (st >= 0) {  // ring of hist_cap records
-    ham_hist[st % hist_cap] = s;
+    ham_hist[st % hist_cap] = red[0];
     t_hist[st % hist_cap] = *tdev;
   }
   *tdev = *tdev + dt;
@@ -118,15 +126,17 @@ static int fail(int code, const char* fmt, ...) {
 namespace {
 
 struct PassCfg {
-  XInvFn xinv = nullptr;
-  XFwdFn xfwd = nullptr;
-  YInvFn yinv = nullptr;
-  YFwdFn yfwd = nullptr;
+  XInvFn xinv[2] = {};
+  XFwdFn xfwd[3] = {};
+  YInvFn yinv[2] = {};
+  YFwdFn yfwd[3] = {};
   int xlines = 1, xthreads = 0;
   size_t xsmem = 0;
-  int ylines = 1, ythreads = 0, ytp = 0;
+  int ylines = 1, ythreads = 0, ylp = 0;
   size_t ysmem = 0;
-  const void* tw = nullptr;
+  const void* twx = nullptr;  // length nx
+  const void* twh = nullptr;  // length ny/2
+  const void* twy = nullptr;  // length ny
 };
 
 int ilog2i(int n) {
@@ -206,12 +216,12 @@ int butcher(int scheme, int* nst, double b[MAX_STAGES][MAX_STAGES], double c[MAX
   }
 }
 
-// exp(-2 pi i k / TW_N), k < TW_N, from long double libm, rounded once.
-std::vector<double2> twiddle_table() {
-  std::vector<double2> t(TW_N);
+// exp(-2 pi i k / n), k < n, from long double libm, rounded once.
+std::vector<double2> twiddle_table(int n) {
+  std::vector<double2> t(n);
   const long double pi = 3.141592653589793238462643383279502884L;
-  for (int k = 0; k < TW_N; k++) {
-    const long double a = 2.0L * pi * (long double)k / (long double)TW_N;
+  for (int k = 0; k < n; k++) {
+    const long double a = 2.0L * pi * (long double)k / (long double)n;
     t[k].x = (double)cosl(a);
     t[k].y = (double)-sinl(a);
   }
@@ -239,8 +249,7 @@ struct hos_ctx {
   double2* ustage = nullptr;
   double2* zplain = nullptr;
   double* pplain = nullptr;
-  double2* tw64 = nullptr;
-  float2* tw32 = nullptr;
+  void* tw[2][3] = {};  // [precision][nx, ny/2, ny] twiddle tables
   double* tdev = nullptr;
   double* trhs = nullptr;
   double* rdev = nullptr;
@@ -280,15 +289,17 @@ struct hos_ctx {
 namespace {
 
 int make_cfg(hos_ctx* c, int prec, PassCfg* o) {
-  o->xinv = lookup_xinv(prec, c->nx);
-  o->xfwd = lookup_xfwd(prec, c->nx);
-  o->yinv = lookup_yinv(prec, c->h);
-  o->yfwd = lookup_yfwd(prec, c->h);
-  if (!o->xinv || !o->xfwd || !o->yinv || !o->yfwd) return fail(HOS_ERR_ARG, "no kernels for %dx%d", c->nx, c->ny);
+  for (int m = 0; m < 2; m++) o->xinv[m] = lookup_xinv(prec, m, c->nx);
+  for (int m = 0; m < 3; m++) o->xfwd[m] = lookup_xfwd(prec, m, c->nx);
+  for (int m = 0; m < 2; m++) o->yinv[m] = lookup_yinv(prec, m, c->h);
+  for (int m = 0; m < 3; m++) o->yfwd[m] = lookup_yfwd(prec, m, c->h);
+  for (int m = 0; m < 3; m++)
+    if (!o->xfwd[m] || !o->yfwd[m] || (m < 2 && (!o->xinv[m] || !o->yinv[m])))
+      return fail(HOS_ERR_ARG, "no kernels for %dx%d", c->nx, c->ny);
   const size_t cs = prec ? sizeof(float2) : sizeof(double2);
   {
     const int E = elems_for(c->nx), P = c->nx / E;
-    int lines = MAX_THREADS / P;
+    int lines = 128 / P;
     if (lines < 1) lines = 1;
     o->xlines = lines;
     o->xthreads = lines * P;
@@ -303,17 +314,23 @@ int make_cfg(hos_ctx* c, int prec, PassCfg* o) {
     o->ythreads = lines * P;
     const int phase = (int)(128 / cs);
     const int target = lines >= phase ? 1 : phase / lines;
-    int tp = c->h + 1;
-    while (tp % phase != target % phase) tp++;
-    o->ytp = tp;
-    o->ysmem = ((size_t)lines * tp + (size_t)lines * (c->h + c->h / E)) * cs;
+    int lp = c->h + c->h / E + 1;
+    while (lp % phase != target % phase) lp++;
+    o->ylp = lp;
+    o->ysmem = (size_t)lines * lp * cs;
   }
   if (o->xthreads % 32 != 0) return fail(HOS_ERR_ARG, "x-pass block of %d threads", o->xthreads);
-  HOS_CK(cudaFuncSetAttribute((const void*)o->xinv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->xsmem));
-  HOS_CK(cudaFuncSetAttribute((const void*)o->xfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->xsmem));
-  HOS_CK(cudaFuncSetAttribute((const void*)o->yinv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->ysmem));
-  HOS_CK(cudaFuncSetAttribute((const void*)o->yfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->ysmem));
-  o->tw = prec ? (const void*)c->tw32 : (const void*)c->tw64;
+  for (int m = 0; m < 2; m++)
+    HOS_CK(cudaFuncSetAttribute((const void*)o->xinv[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->xsmem));
+  for (int m = 0; m < 3; m++)
+    HOS_CK(cudaFuncSetAttribute((const void*)o->xfwd[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->xsmem));
+  for (int m = 0; m < 2; m++)
+    HOS_CK(cudaFuncSetAttribute((const void*)o->yinv[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->ysmem));
+  for (int m = 0; m < 3; m++)
+    HOS_CK(cudaFuncSetAttribute((const void*)o->yfwd[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->ysmem));
+  o->twx = c->tw[prec][0];
+  o->twh = c->tw[prec][1];
+  o->twy = c->tw[prec][2];
   return HOS_OK;
 }
 
@@ -331,23 +348,52 @@ size_t compute_bytes(const hos_params* p, int nst) {
   b += (size_t)(4 + M) * fsz * cs;                   // Z / V scratch
   b += (size_t)(5 + M * (M + 1) / 2 + L) * psz * rs; // physical fields
   b += 2 * fsz * 16 + fsz * 16 + 2 * psz * 8;        // boundary scratch (FP64)
-  b += (size_t)TW_N * (16 + 8);
+  b += (nx + h + ny) * (16 + 8);
   b += 2 * (size_t)HIST_CAP * 8 + 4096 * 8 + 4096;
   return b;
 }
 
+// Optional per-pass recorder: an event after every launch, with the pass
+// kind and its algorithmic bytes (compulsory reads + writes of that pass).
+struct PassLog {
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> kind;
+  std::vector<double> bytes;
+  int act_rows = 0;
+};
+
+enum PassKind { P_XINV_STAGE, P_YINV_STAGE, P_YFWD_LEVEL, P_XFWD_LEVEL, P_YINV_LEVEL, P_YFWD_RHS, P_XFWD_RHS, P_NKIND };
+const char* pass_name(int k) {
+  static const char* names[P_NKIND] = {"xinv_stage", "yinv_stage", "yfwd_level", "xfwd_level",
+                                       "yinv_level", "yfwd_rhs",   "xfwd_rhs"};
+  return (k >= 0 && k < P_NKIND) ? names[k] : "?";
+}
+
+void log_pass(hos_ctx* c, PassLog* lg, int kind, double bytes) {
+  if (!lg) return;
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  cudaEventRecord(e, c->st);
+  lg->ev.push_back(e);
+  lg->kind.push_back(kind);
+  lg->bytes.push_back(bytes);
+}
+
 // Enqueues one RK stage (or one bare RHS evaluation when rhs_only).
 int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, double2* kout, const double* tsrc,
-                  const int* rows_dev) {
+                  const int* rows_dev, PassLog* lg = nullptr) {
   const PassCfg& g = c->cfg;
   const int M = c->M, L = c->L;
   const size_t fsz = c->fsz;
   const size_t cs = c->prec ? sizeof(float2) : sizeof(double2);
+  const size_t rs = c->prec ? sizeof(float) : sizeof(double);
   char* zb = reinterpret_cast<char*>(c->zbuf);
+  const double act = lg ? (double)lg->act_rows : 0.0;
+  const double nxd = (double)c->nx, psz = (double)c->psz, fszd = (double)fsz, my = (double)c->geo.my;
+  const int gx = xgrid(c, g), gy = ygrid(c, g);
 
   XInvArgs xa{};
   xa.geo = c->geo;
-  xa.mode = 0;
   xa.rows = c->h + 1;
   xa.rows_dev = rows_dev;
   xa.u = uin;
@@ -360,18 +406,18 @@ int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, dou
     }
   }
   xa.nk = nk;
-  xa.ndz = M;
   xa.z = c->zbuf;
   xa.tdev = tsrc;
   xa.rdev = c->rdev;
   xa.set_ramp = (s == 0);
   xa.tramp = c->p.tramp;
   xa.rampflg = c->p.rampflg;
-  g.xinv<<<xgrid(c, g), g.xthreads, g.xsmem, c->st>>>(xa, g.tw);
+  g.xinv[XI_STAGE]<<<dim3(gx, 4 + M), g.xthreads, g.xsmem, c->st>>>(xa, g.twx);
+  log_pass(c, lg, P_XINV_STAGE, act * nxd * (16.0 * 2 * (1 + nk) + (double)cs * (4 + M)));
 
   YInvArgs ya{};
   ya.geo = c->geo;
-  ya.tp = g.ytp;
+  ya.lp = g.ylp;
   ya.z = c->zbuf;
   ya.rows_in = c->h + 1;
   ya.rows_dev = rows_dev;
@@ -383,15 +429,13 @@ int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, dou
   ya.jobs[nj++] = YJob{2, 1, c->PHIY()};
   ya.jobs[nj++] = YJob{3, 0, c->PHIX()};
   for (int j = 1; j <= M; j++) ya.jobs[nj++] = YJob{4 + j - 1, 0, c->D(1, j)};
-  ya.njobs = nj;
-  ya.wmode = 0;
-  g.yinv<<<ygrid(c, g), g.ythreads, g.ysmem, c->st>>>(ya, g.tw);
+  g.yinv[YI_JOBS]<<<dim3(gy, nj), g.ythreads, g.ysmem, c->st>>>(ya, g.twh, g.twy);
+  log_pass(c, lg, P_YINV_STAGE, act * nxd * (double)cs * (4 + M) + psz * (double)rs * (5 + M));
 
   for (int n = 1; n <= L; n++) {
     YFwdArgs fa{};
     fa.geo = c->geo;
-    fa.tp = g.ytp;
-    fa.mode = 1;
+    fa.lp = g.ylp;
     fa.phys = c->phys;
     fa.eta = c->ETA();
     fa.nterms = n;
@@ -401,27 +445,26 @@ int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, dou
     }
     fa.vout = zb;
     fa.rows_out = c->h + 1;
-    g.yfwd<<<ygrid(c, g), g.ythreads, g.ysmem, c->st>>>(fa, g.tw);
+    g.yfwd[YF_LEVEL]<<<dim3(gy, 1), g.ythreads, g.ysmem, c->st>>>(fa, g.twh, g.twy);
+    log_pass(c, lg, P_YFWD_LEVEL, psz * (double)rs * (n + 1) + fszd * (double)cs);
 
     XFwdArgs xf{};
     xf.geo = c->geo;
-    xf.mode = 1;
     xf.rows = c->h + 1;
     xf.vin0 = zb;
     xf.zout = zb + fsz * cs;
     xf.ndz = M - n;
-    g.xfwd<<<xgrid(c, g), g.xthreads, g.xsmem, c->st>>>(xf, g.tw);
+    g.xfwd[XF_LEVEL]<<<dim3(gx, 1), g.xthreads, g.xsmem, c->st>>>(xf, g.twx);
+    log_pass(c, lg, P_XFWD_LEVEL, fszd * (double)cs * (1 + M - n));
 
     YInvArgs yl{};
     yl.geo = c->geo;
-    yl.tp = g.ytp;
+    yl.lp = g.ylp;
     yl.z = c->zbuf;
     yl.rows_in = c->h + 1;
     yl.phys = c->phys;
     int nl = 0;
     for (int j = 1; j <= M - n; j++) yl.jobs[nl++] = YJob{1 + j - 1, 0, c->D(n + 1, j)};
-    yl.njobs = nl;
-    yl.wmode = 1;
     yl.w_out = c->W(n);
     yl.eta = c->ETA();
     yl.w_terms = n;
@@ -429,13 +472,13 @@ int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, dou
       yl.w_in[m] = c->D(m + 1, n - m + 1);
       yl.w_pow[m] = n - m;
     }
-    g.yinv<<<ygrid(c, g), g.ythreads, g.ysmem, c->st>>>(yl, g.tw);
+    g.yinv[YI_LEVEL]<<<dim3(gy, nl), g.ythreads, g.ysmem, c->st>>>(yl, g.twh, g.twy);
+    log_pass(c, lg, P_YINV_LEVEL, fszd * (double)cs * (M - n) + psz * (double)rs * (M - n + 1 + n + 1));
   }
 
   YFwdArgs ff{};
   ff.geo = c->geo;
-  ff.tp = g.ytp;
-  ff.mode = 2;
+  ff.lp = g.ylp;
   ff.phys = c->phys;
   ff.ex = c->ETAX();
   ff.ey = c->ETAY();
@@ -445,11 +488,11 @@ int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, dou
   for (int n = 0; n <= L; n++) ff.w_idx[n] = c->W(n);
   ff.vout = zb;
   ff.rows_out = c->geo.my;
-  g.yfwd<<<ygrid(c, g), g.ythreads, g.ysmem, c->st>>>(ff, g.tw);
+  g.yfwd[YF_RHS]<<<dim3(gy, 2), g.ythreads, g.ysmem, c->st>>>(ff, g.twh, g.twy);
+  log_pass(c, lg, P_YFWD_RHS, psz * (double)rs * (5 + L) + 2.0 * my * nxd * (double)cs);
 
   XFwdArgs xe{};
   xe.geo = c->geo;
-  xe.mode = 2;
   xe.rows = c->h + 1;
   xe.rows_dev = rows_dev;
   xe.rows_fft = c->geo.my;
@@ -471,8 +514,14 @@ int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, dou
     xe.cfin[p] = dt * c->c[p];
   }
   xe.nstage = c->nst;
-  xe.unew = uin;
-  g.xfwd<<<xgrid(c, g), g.xthreads, g.xsmem, c->st>>>(xe, g.tw);
+  g.xfwd[XF_RHS]<<<dim3(gx, 2), g.xthreads, g.xsmem, c->st>>>(xe, g.twx);
+  {
+    // V rows < my in, stage input (u + earlier k) rows < act, k_s rows < my out;
+    // on the last stage also the other k's and the updated u (rows < my)
+    double b = 2.0 * my * nxd * (double)cs + act * nxd * 16.0 * 2 * (1 + nk) + my * nxd * 16.0 * 2;
+    if (xe.final_update) b += my * nxd * 16.0 * 2 * (c->nst - 1) + my * nxd * 16.0 * 2;
+    log_pass(c, lg, P_XFWD_RHS, b);
+  }
   return HOS_OK;
 }
 
@@ -481,7 +530,7 @@ int enqueue_step(hos_ctx* c, double dt) {
     int rc = enqueue_stage(c, s, dt, false, c->u, c->k + (size_t)s * 2 * c->fsz, c->tdev, c->actdev);
     if (rc) return rc;
   }
-  k_step_end<<<1, 32, 0, c->st>>>(c->ham_part, xgrid(c, c->cfg), c->tdev, dt, c->stepdev, c->ham_hist, c->t_hist,
+  k_step_end<<<1, 256, 0, c->st>>>(c->ham_part, xgrid(c, c->cfg), c->tdev, dt, c->stepdev, c->ham_hist, c->t_hist,
                                   HIST_CAP);
   return HOS_OK;
 }
@@ -518,20 +567,18 @@ int enqueue_r2c(hos_ctx* c, const double* phys_in, double2* spec_out, int dealia
   const PassCfg& g = c->cfg64;
   YFwdArgs fa{};
   fa.geo = c->geo;
-  fa.tp = g.ytp;
-  fa.mode = 0;
+  fa.lp = g.ylp;
   fa.in_ptr = phys_in;
   fa.vout = c->zplain;
   fa.rows_out = c->h + 1;
-  g.yfwd<<<ygrid(c, g), g.ythreads, g.ysmem, c->st>>>(fa, g.tw);
+  g.yfwd[YF_PLAIN]<<<dim3(ygrid(c, g), 1), g.ythreads, g.ysmem, c->st>>>(fa, g.twh, g.twy);
   XFwdArgs xf{};
   xf.geo = c->geo;
-  xf.mode = 0;
   xf.rows = c->h + 1;
   xf.vin0 = c->zplain;
   xf.out_spec = spec_out;
   xf.dealias = dealias;
-  g.xfwd<<<xgrid(c, g), g.xthreads, g.xsmem, c->st>>>(xf, g.tw);
+  g.xfwd[XF_PLAIN]<<<dim3(xgrid(c, g), 1), g.xthreads, g.xsmem, c->st>>>(xf, g.twx);
   return HOS_OK;
 }
 
@@ -539,23 +586,18 @@ int enqueue_c2r(hos_ctx* c, const double2* spec_in, double* phys_out) {
   const PassCfg& g = c->cfg64;
   XInvArgs xa{};
   xa.geo = c->geo;
-  xa.mode = 1;
   xa.rows = c->h + 1;
   xa.u = spec_in;
   xa.z = c->zplain;
-  xa.tdev = c->tdev;
-  xa.rdev = c->rdev;
-  xa.set_ramp = 0;
-  g.xinv<<<xgrid(c, g), g.xthreads, g.xsmem, c->st>>>(xa, g.tw);
+  g.xinv[XI_PLAIN]<<<dim3(xgrid(c, g), 1), g.xthreads, g.xsmem, c->st>>>(xa, g.twx);
   YInvArgs ya{};
   ya.geo = c->geo;
-  ya.tp = g.ytp;
+  ya.lp = g.ylp;
   ya.z = c->zplain;
   ya.rows_in = c->h + 1;
   ya.phys = phys_out;
   ya.jobs[0] = YJob{0, 0, 0};
-  ya.njobs = 1;
-  g.yinv<<<ygrid(c, g), g.ythreads, g.ysmem, c->st>>>(ya, g.tw);
+  g.yinv[YI_JOBS]<<<dim3(ygrid(c, g), 1), g.ythreads, g.ysmem, c->st>>>(ya, g.twh, g.twy);
   return HOS_OK;
 }
 
@@ -570,9 +612,9 @@ void release(hos_ctx* c) {
   if (!c) return;
   if (c->gexec) cudaGraphExecDestroy(c->gexec);
   if (c->graph) cudaGraphDestroy(c->graph);
-  void* ptrs[] = {c->u,      c->k,    c->zbuf, c->phys,    c->ustage, c->zplain, c->pplain,   c->tw64,
-                  c->tw32,   c->tdev, c->trhs, c->rdev,    c->stepdev, c->actdev, c->flagdev, c->ham_part,
-                  c->ham_hist, c->t_hist};
+  void* ptrs[] = {c->u,    c->k,    c->zbuf,    c->phys,   c->ustage, c->zplain,   c->pplain,
+                  c->tdev, c->trhs, c->rdev,    c->stepdev, c->actdev, c->flagdev, c->ham_part,
+                  c->ham_hist, c->t_hist, c->tw[0][0], c->tw[0][1], c->tw[0][2], c->tw[1][0], c->tw[1][1], c->tw[1][2]};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->st) cudaStreamDestroy(c->st);
@@ -691,8 +733,13 @@ int hos_create(const hos_params* p, hos_handle* out) {
   HOS_AL(c->ustage, 2 * c->fsz * sizeof(double2));
   HOS_AL(c->zplain, c->fsz * sizeof(double2));
   HOS_AL(c->pplain, 2 * c->psz * sizeof(double));
-  HOS_AL(c->tw64, TW_N * sizeof(double2));
-  HOS_AL(c->tw32, TW_N * sizeof(float2));
+  {
+    const int lens[3] = {c->nx, c->h, c->ny};
+    for (int q = 0; q < 3; q++) {
+      HOS_AL(c->tw[0][q], (size_t)lens[q] * sizeof(double2));
+      HOS_AL(c->tw[1][q], (size_t)lens[q] * sizeof(float2));
+    }
+  }
   HOS_AL(c->tdev, sizeof(double));
   HOS_AL(c->trhs, sizeof(double));
   HOS_AL(c->rdev, sizeof(double));
@@ -715,11 +762,17 @@ int hos_create(const hos_params* p, hos_handle* out) {
     return rc;
   }
   // twiddles, zeroed state and stage buffers (rows ky >= my of k are never written)
-  std::vector<double2> tw = twiddle_table();
-  std::vector<float2> tw32(TW_N);
-  for (int i = 0; i < TW_N; i++) tw32[i] = make_float2((float)tw[i].x, (float)tw[i].y);
-  e = cudaMemcpy(c->tw64, tw.data(), TW_N * sizeof(double2), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(c->tw32, tw32.data(), TW_N * sizeof(float2), cudaMemcpyHostToDevice);
+  e = cudaSuccess;
+  {
+    const int lens[3] = {c->nx, c->h, c->ny};
+    for (int q = 0; q < 3 && e == cudaSuccess; q++) {
+      std::vector<double2> tw = twiddle_table(lens[q]);
+      std::vector<float2> tw32(lens[q]);
+      for (int i = 0; i < lens[q]; i++) tw32[i] = make_float2((float)tw[i].x, (float)tw[i].y);
+      e = cudaMemcpy(c->tw[0][q], tw.data(), lens[q] * sizeof(double2), cudaMemcpyHostToDevice);
+      if (e == cudaSuccess) e = cudaMemcpy(c->tw[1][q], tw32.data(), lens[q] * sizeof(float2), cudaMemcpyHostToDevice);
+    }
+  }
   if (e == cudaSuccess) e = cudaMemsetAsync(c->u, 0, 2 * c->fsz * sizeof(double2), c->st);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->k, 0, (size_t)c->nst * 2 * c->fsz * sizeof(double2), c->st);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->tdev, 0, sizeof(double), c->st);
@@ -897,6 +950,56 @@ int hos_check_finite(hos_handle h, int* finite) {
   HOS_CK(cudaStreamSynchronize(h->st));
   *finite = f ? 0 : 1;
   return HOS_OK;
+}
+
+int hos_profile_stage(hos_handle h, double dt, int reps, hos_pass_stat* out, int max, int* count) {
+  if (!h || !out || !count || reps < 1) return fail(HOS_ERR_ARG, "bad argument");
+  // stage 1 of an RK step from the resident state, written to scratch: the
+  // state, t and the energy record are untouched
+  HOS_CK(cudaMemcpyAsync(h->ustage, h->u, 2 * h->fsz * sizeof(double2), cudaMemcpyDeviceToDevice, h->st));
+  HOS_CK(cudaMemcpyAsync(h->trhs, h->tdev, sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+  int act = 0;
+  HOS_CK(cudaMemcpyAsync(&act, h->actdev, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  HOS_CK(cudaStreamSynchronize(h->st));
+  const int s = h->nst > 1 ? 1 : 0;
+  double2* kout = h->k + (size_t)(h->nst - 1) * 2 * h->fsz;
+  std::vector<double> ms(P_NKIND, 0.0), by(P_NKIND, 0.0);
+  std::vector<int> n(P_NKIND, 0);
+  for (int r = 0; r < reps; r++) {
+    PassLog lg;
+    lg.act_rows = act;
+    log_pass(h, &lg, -1, 0.0);
+    int rc = enqueue_stage(h, s, dt, true, h->ustage, kout, h->trhs, h->actdev, &lg);
+    if (rc) return rc;
+    HOS_CK(cudaStreamSynchronize(h->st));
+    for (size_t i = 1; i < lg.ev.size(); i++) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, lg.ev[i - 1], lg.ev[i]);
+      const int k = lg.kind[i];
+      ms[k] += t;
+      by[k] += lg.bytes[i];
+      if (r == 0) n[k]++;
+    }
+    for (cudaEvent_t e : lg.ev) cudaEventDestroy(e);
+  }
+  int c = 0;
+  for (int k = 0; k < P_NKIND && c < max; k++) {
+    if (!n[k]) continue;
+    std::memset(&out[c], 0, sizeof(out[c]));
+    std::strncpy(out[c].name, pass_name(k), sizeof(out[c].name) - 1);
+    out[c].launches_per_stage = n[k];
+    out[c].ms_per_launch = ms[k] / (reps * n[k]);
+    out[c].bytes_per_launch = by[k] / (reps * n[k]);
+    c++;
+  }
+  *count = c;
+  HOS_CK(cudaGetLastError());
+  return HOS_OK;
+}
+
+int hos_launches_per_step(hos_handle h) {
+  if (!h) return -1;
+  return h->nst * (4 + 3 * h->L) + 1;
 }
 
 int hos_volume(hos_handle h, double* vol) {

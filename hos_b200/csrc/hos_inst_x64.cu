@@ -3,27 +3,45 @@
 
 namespace hos {
 
-#define HOS_X_CASE(N) \
-  case N:             \
-    return &k_xinv<double, N, elems_for(N)>;
-XInvFn lookup_xinv_64(int n) {
+#define HOS_SIZES(F) F(16) F(32) F(64) F(128) F(256) F(512) F(1024) F(2048) F(4096)
+
+#define HOS_CASE(N) \
+  case N:           \
+    return &k_xinv<double, N, elems_for(N), M>;
+template <int M>
+static XInvFn xinv_n(int n) {
   switch (n) {
-    HOS_X_CASE(16) HOS_X_CASE(32) HOS_X_CASE(64) HOS_X_CASE(128) HOS_X_CASE(256) HOS_X_CASE(512)
-    HOS_X_CASE(1024) HOS_X_CASE(2048) HOS_X_CASE(4096)
+    HOS_SIZES(HOS_CASE)
     default: return nullptr;
   }
 }
-#undef HOS_X_CASE
-#define HOS_X_CASE(N) \
-  case N:             \
-    return &k_xfwd<double, N, elems_for(N)>;
-XFwdFn lookup_xfwd_64(int n) {
+#undef HOS_CASE
+#define HOS_CASE(N) \
+  case N:           \
+    return &k_xfwd<double, N, elems_for(N), M>;
+template <int M>
+static XFwdFn xfwd_n(int n) {
   switch (n) {
-    HOS_X_CASE(16) HOS_X_CASE(32) HOS_X_CASE(64) HOS_X_CASE(128) HOS_X_CASE(256) HOS_X_CASE(512)
-    HOS_X_CASE(1024) HOS_X_CASE(2048) HOS_X_CASE(4096)
+    HOS_SIZES(HOS_CASE)
     default: return nullptr;
   }
 }
-#undef HOS_X_CASE
+#undef HOS_CASE
+
+XInvFn lookup_xinv_64(int mode, int n) {
+  switch (mode) {
+    case XI_STAGE: return xinv_n<XI_STAGE>(n);
+    case XI_PLAIN: return xinv_n<XI_PLAIN>(n);
+    default: return nullptr;
+  }
+}
+XFwdFn lookup_xfwd_64(int mode, int n) {
+  switch (mode) {
+    case XF_PLAIN: return xfwd_n<XF_PLAIN>(n);
+    case XF_LEVEL: return xfwd_n<XF_LEVEL>(n);
+    case XF_RHS: return xfwd_n<XF_RHS>(n);
+    default: return nullptr;
+  }
+}
 
 }  // namespace hos

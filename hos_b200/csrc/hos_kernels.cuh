@@ -12,7 +12,13 @@
 //
 // x-passes read and write whole rows with consecutive threads on consecutive
 // addresses.  y-passes own G consecutive x rows; their spectral side is read
-// or written as G-wide column strips staged through a shared-memory tile.
+// or written as G-wide column strips staged through shared memory, in the
+// same buffer the line FFT then uses for its exchanges.
+//
+// Kernels are specialised per mode (so each mode gets its own register
+// allocation) and most take one output per block along gridDim.y, which
+// keeps many small blocks resident per SM; inputs that several outputs share
+// are re-read from L2.
 //
 // The spectral multipliers, the RK stage input, the Taylor products of the
 // vertical-velocity recursion, the RHS assembly, the Dommermuth ramp, the
@@ -49,33 +55,40 @@ __device__ __forceinline__ bool keep_mode(const Geo& G, int i, int j) {
 }
 // Multiplier of the p-th z-derivative: kz^p (deep water, operators_par.c:168-192);
 // finite depth: kz^p * tanh(kz h) for odd p.
-__device__ __forceinline__ double dz_mult(double kz, double th, int p) {
+__device__ __forceinline__ double dz_mult(const Geo& G, double kz, int p) {
   double m = 1.0;
   for (int q = 0; q < p; q++) m *= kz;
-  return (p & 1) ? m * th : m;
+  if ((p & 1) && G.depth > 0) m *= tanh(kz * G.depth);
+  return m;
 }
+
+enum { XI_STAGE = 0, XI_PLAIN = 1 };
+enum { XF_PLAIN = 0, XF_LEVEL = 1, XF_RHS = 2 };
+enum { YI_JOBS = 0, YI_LEVEL = 1 };
+enum { YF_PLAIN = 0, YF_LEVEL = 1, YF_RHS = 2 };
 
 // ---------------------------------------------------------------- x inverse
 struct XInvArgs {
   Geo geo;
-  int mode;  // 0: RK stage (4 + ndz outputs); 1: plain c2r x-pass of one field
-  int rows;  // ky rows that may be nonzero in the input
+  int rows;             // ky rows that may be nonzero in the input
   const int* rows_dev;  // if set, overrides rows (active rows of the state, kept on the device)
-  const double2* u;                 // stage: packed state [2][h+1][nx]; plain: one field
-  const double2* kp[MAX_STAGES];    // earlier stage derivatives
-  double coef[MAX_STAGES];          // dt*b[s][p]
+  const double2* u;     // STAGE: packed state [2][h+1][nx]; PLAIN: one field
+  const double2* kp[MAX_STAGES];  // earlier stage derivatives
+  double coef[MAX_STAGES];        // dt*b[s][p]
   int nk;
-  int ndz;                          // number of z-derivative outputs (orders 1..ndz)
-  void* z;                          // output complex arrays, stride (h+1)*nx
-  const double* tdev;               // simulation time (device)
-  double* rdev;                     // ramp factor for this step (device), written if set_ramp
+  void* z;              // output complex arrays (T2), stride (h+1)*nx; output o = blockIdx.y
+  const double* tdev;   // simulation time (device)
+  double* rdev;         // ramp factor for this step (device), written if set_ramp
   int set_ramp;
   double tramp;
   int rampflg;
 };
 
-template <typename T, int NX, int E>
-__global__ void __launch_bounds__(MAX_THREADS) k_xinv(const __grid_constant__ XInvArgs a, const void* twv) {
+// STAGE outputs (blockIdx.y = o): 0 eta, 1 i kx eta, 2 phi, 3 i kx phi,
+// 3+p d_z^p phi (p >= 1).  The stage input u + sum coef*k is formed on the
+// fly (time_schemes_par.c:38-67).
+template <typename T, int NX, int E, int MODE>
+__global__ void __launch_bounds__(MAX_THREADS, 2) k_xinv(const __grid_constant__ XInvArgs a, const void* twv) {
   using C = cpx<T>;
   constexpr int P = NX / E;
   const C* tw = reinterpret_cast<const C*>(twv);
@@ -86,13 +99,11 @@ __global__ void __launch_bounds__(MAX_THREADS) k_xinv(const __grid_constant__ XI
   const int lines = blockDim.x / P;
   const int row = blockIdx.x * lines + line;
   const int rows = a.rows_dev ? *a.rows_dev : a.rows;
-  const bool live = row < rows;
   const Geo& geo = a.geo;
   const size_t fsz = (size_t)(geo.h + 1) * NX;
-  const size_t roff = (size_t)(live ? row : 0) * NX;
-  C* z = reinterpret_cast<C*>(a.z);
+  const int o = blockIdx.y;
 
-  if (a.set_ramp && blockIdx.x == 0 && threadIdx.x == 0) {
+  if (MODE == XI_STAGE && a.set_ramp && blockIdx.x == 0 && o == 0 && threadIdx.x == 0) {
     double r = 1.0;
     if (a.rampflg == 1) {
       const double tt = *a.tdev;
@@ -101,147 +112,81 @@ __global__ void __launch_bounds__(MAX_THREADS) k_xinv(const __grid_constant__ XI
     *a.rdev = r;
   }
   if ((int)(blockIdx.x * lines) >= rows) return;  // whole block beyond the active rows
+  const bool live = row < rows;
+  const size_t roff = (size_t)(live ? row : 0) * NX;
+  C* z = reinterpret_cast<C*>(a.z) + (size_t)o * fsz;
 
   C v[E];
-  if (a.mode == 1) {
+  if (MODE == XI_PLAIN) {
 #pragma unroll
     for (int e = 0; e < E; e++) v[e] = live ? conv<T>(a.u[roff + t + e * P]) : mkc((T)0, (T)0);
-    line_fft<T, NX, E, true>(v, sm, t, tw);
-    if (live) {
+  } else {
+    const size_t foff = (o < 2) ? 0 : fsz;
+    const double ky = ky_of(geo, row);
 #pragma unroll
-      for (int e = 0; e < E; e++) z[roff + t + e * P] = v[e];
-    }
-    return;
-  }
-
-  const double ky = ky_of(geo, row);
-  double2 w[E];
-  // ---- eta: stage input (time_schemes_par.c:38-67)
-#pragma unroll
-  for (int e = 0; e < E; e++) {
-    double2 x = make_double2(0.0, 0.0);
-    if (live) {
-      const size_t idx = roff + t + e * P;
-      x = a.u[idx];
-      for (int p = 0; p < a.nk; p++) {
-        const double2 kk = a.kp[p][idx];
-        x.x = x.x + a.coef[p] * kk.x;
-        x.y = x.y + a.coef[p] * kk.y;
+    for (int e = 0; e < E; e++) {
+      double2 x = make_double2(0.0, 0.0);
+      const int i = t + e * P;
+      if (live) {
+        const size_t idx = foff + roff + i;
+        x = a.u[idx];
+        for (int p = 0; p < a.nk; p++) {
+          const double2 kk = a.kp[p][idx];
+          x.x = x.x + a.coef[p] * kk.x;
+          x.y = x.y + a.coef[p] * kk.y;
+        }
       }
+      if (o == 1 || o == 3) {  // Dx: i kx (operators_par.c:66)
+        const double kx = kx_of(geo, i);
+        x = make_double2(-kx * x.y, kx * x.x);
+      } else if (o >= 4) {  // Dz applied o-3 times (operators_par.c:168-192)
+        const double kx = kx_of(geo, i);
+        const double m = dz_mult(geo, sqrt(kx * kx + ky * ky), o - 3);
+        x = make_double2(m * x.x, m * x.y);
+      }
+      v[e] = conv<T>(x);
     }
-    w[e] = x;
   }
-  // out 0: eta
-#pragma unroll
-  for (int e = 0; e < E; e++) v[e] = conv<T>(w[e]);
   line_fft<T, NX, E, true>(v, sm, t, tw);
   if (live) {
 #pragma unroll
     for (int e = 0; e < E; e++) z[roff + t + e * P] = v[e];
-  }
-  // out 1: i kx eta (Dx, operators_par.c:66)
-#pragma unroll
-  for (int e = 0; e < E; e++) {
-    const double kx = kx_of(geo, t + e * P);
-    v[e] = conv<T>(make_double2(-kx * w[e].y, kx * w[e].x));
-  }
-  line_fft<T, NX, E, true>(v, sm, t, tw);
-  if (live) {
-#pragma unroll
-    for (int e = 0; e < E; e++) z[fsz + roff + t + e * P] = v[e];
-  }
-  // ---- phi stage input
-#pragma unroll
-  for (int e = 0; e < E; e++) {
-    double2 x = make_double2(0.0, 0.0);
-    if (live) {
-      const size_t idx = fsz + roff + t + e * P;
-      x = a.u[idx];
-      for (int p = 0; p < a.nk; p++) {
-        const double2 kk = a.kp[p][idx];
-        x.x = x.x + a.coef[p] * kk.x;
-        x.y = x.y + a.coef[p] * kk.y;
-      }
-    }
-    w[e] = x;
-  }
-  // out 2: phi (its y-derivative is taken in the y-pass)
-#pragma unroll
-  for (int e = 0; e < E; e++) v[e] = conv<T>(w[e]);
-  line_fft<T, NX, E, true>(v, sm, t, tw);
-  if (live) {
-#pragma unroll
-    for (int e = 0; e < E; e++) z[2 * fsz + roff + t + e * P] = v[e];
-  }
-  // out 3: i kx phi
-#pragma unroll
-  for (int e = 0; e < E; e++) {
-    const double kx = kx_of(geo, t + e * P);
-    v[e] = conv<T>(make_double2(-kx * w[e].y, kx * w[e].x));
-  }
-  line_fft<T, NX, E, true>(v, sm, t, tw);
-  if (live) {
-#pragma unroll
-    for (int e = 0; e < E; e++) z[3 * fsz + roff + t + e * P] = v[e];
-  }
-  // out 4..: z-derivatives of phi of orders 1..ndz (Dz, operators_par.c:168-192)
-  double kz[E], th[E];
-#pragma unroll
-  for (int e = 0; e < E; e++) {
-    const double kx = kx_of(geo, t + e * P);
-    kz[e] = sqrt(kx * kx + ky * ky);
-    th[e] = geo.depth > 0 ? tanh(kz[e] * geo.depth) : 1.0;
-  }
-  for (int p = 1; p <= a.ndz; p++) {
-#pragma unroll
-    for (int e = 0; e < E; e++) {
-      const double m = dz_mult(kz[e], th[e], p);
-      v[e] = conv<T>(make_double2(m * w[e].x, m * w[e].y));
-    }
-    line_fft<T, NX, E, true>(v, sm, t, tw);
-    if (live) {
-#pragma unroll
-      for (int e = 0; e < E; e++) z[(size_t)(3 + p) * fsz + roff + t + e * P] = v[e];
-    }
   }
 }
 
 // ---------------------------------------------------------------- x forward
 struct XFwdArgs {
   Geo geo;
-  int mode;       // 0: plain r2c x-pass -> FP64 spectral; 1: level (forward, then ndz inverse outputs); 2: RK stage end
-  int rows;       // rows processed
+  int rows;             // rows processed
   const int* rows_dev;  // if set, overrides rows
-  int rows_fft;   // mode 2: rows < rows_fft are transformed; rows in [rows_fft, rows) only add to the Hamiltonian
-  const void* vin0;  // input V arrays (T2) [h+1][nx]
+  int rows_fft;         // RHS: rows < rows_fft are transformed; rows in [rows_fft, rows) only add to the Hamiltonian
+  const void* vin0;     // input V arrays (T2) [h+1][nx]; RHS: blockIdx.y selects vin0 (eta) or vin1 (phi)
   const void* vin1;
-  double2* out_spec;  // mode 0 output
-  int dealias;        // mode 0: zero the modes Dealias zeroes (operators_par.c:283-325)
-  void* zout;         // mode 1: output Z arrays (T2), stride (h+1)*nx
-  int ndz;
-  // mode 2
-  const double2* u;               // packed state at step start (updated in place on the final stage)
+  double2* out_spec;    // PLAIN output
+  int dealias;          // PLAIN: zero the modes Dealias zeroes (operators_par.c:283-325)
+  void* zout;           // LEVEL: output Z arrays (T2), stride (h+1)*nx
+  int ndz;              // LEVEL: z-derivative orders 1..ndz
+  // RHS
+  double2* u;                     // packed state at step start (updated in place on the final stage)
   const double2* kp[MAX_STAGES];  // earlier stage derivatives (stage input = u + sum coef*kp)
   double coef[MAX_STAGES];
   int nk;
   double2* kout;                  // this stage's derivative [2][h+1][nx]
   const double* rdev;             // ramp factor
   int ham;                        // accumulate the stage-0 Hamiltonian
-  double* ham_part;               // one partial per block
+  double* ham_part;               // one partial per block of the eta half
   int final_update;               // u += sum cfin[s] * k_s (time_schemes_par.c:98-116)
   const double2* kall[MAX_STAGES];
   double cfin[MAX_STAGES];
   int nstage;                     // number of stages; k of the last one is in registers
-  double2* unew;
 };
 
-template <typename T, int NX, int E>
-__global__ void __launch_bounds__(MAX_THREADS) k_xfwd(const __grid_constant__ XFwdArgs a, const void* twv) {
+template <typename T, int NX, int E, int MODE>
+__global__ void __launch_bounds__(MAX_THREADS, 2) k_xfwd(const __grid_constant__ XFwdArgs a, const void* twv) {
   using C = cpx<T>;
   constexpr int P = NX / E;
   const C* tw = reinterpret_cast<const C*>(twv);
   extern __shared__ __align__(16) unsigned char smraw[];
-  __shared__ double red[MAX_THREADS / 32];
   const int line = threadIdx.x / P;
   const int t = threadIdx.x - line * P;
   C* sm = reinterpret_cast<C*>(smraw) + line * line_smem_elems<NX, E>();
@@ -249,9 +194,9 @@ __global__ void __launch_bounds__(MAX_THREADS) k_xfwd(const __grid_constant__ XF
   const int row = blockIdx.x * lines + line;
   const Geo& geo = a.geo;
   const size_t fsz = (size_t)(geo.h + 1) * NX;
-  const T sc = (T)geo.inv_nxny;
 
-  if (a.mode != 2) {
+  if (MODE != XF_RHS) {
+    const T sc = (T)geo.inv_nxny;
     const bool live = row < a.rows;
     const size_t roff = (size_t)(live ? row : 0) * NX;
     const C* vin = reinterpret_cast<const C*>(a.vin0);
@@ -261,7 +206,7 @@ __global__ void __launch_bounds__(MAX_THREADS) k_xfwd(const __grid_constant__ XF
     line_fft<T, NX, E, false>(v, sm, t, tw);
 #pragma unroll
     for (int e = 0; e < E; e++) v[e] = cscale(v[e], sc);  // fft_2d's 1/Nx/Ny (exact: powers of two)
-    if (a.mode == 0) {
+    if (MODE == XF_PLAIN) {
       if (live) {
 #pragma unroll
         for (int e = 0; e < E; e++) {
@@ -271,20 +216,16 @@ __global__ void __launch_bounds__(MAX_THREADS) k_xfwd(const __grid_constant__ XF
       }
       return;
     }
-    // mode 1: phi^(n+1) hat is in v; emit its z-derivatives of orders 1..ndz
+    // LEVEL: v holds phi^(n+1) hat; emit its z-derivatives of orders 1..ndz
     const double ky = ky_of(geo, row);
-    double kz[E], th[E];
-#pragma unroll
-    for (int e = 0; e < E; e++) {
-      const double kx = kx_of(geo, t + e * P);
-      kz[e] = sqrt(kx * kx + ky * ky);
-      th[e] = geo.depth > 0 ? tanh(kz[e] * geo.depth) : 1.0;
-    }
     C* z = reinterpret_cast<C*>(a.zout);
     for (int p = 1; p <= a.ndz; p++) {
       C w[E];
 #pragma unroll
-      for (int e = 0; e < E; e++) w[e] = cscale(v[e], (T)dz_mult(kz[e], th[e], p));
+      for (int e = 0; e < E; e++) {
+        const double kx = kx_of(geo, t + e * P);
+        w[e] = cscale(v[e], (T)dz_mult(geo, sqrt(kx * kx + ky * ky), p));
+      }
       line_fft<T, NX, E, true>(w, sm, t, tw);
       if (live) {
 #pragma unroll
@@ -294,93 +235,77 @@ __global__ void __launch_bounds__(MAX_THREADS) k_xfwd(const __grid_constant__ XF
     return;
   }
 
-  // ---- mode 2: end of an RK stage (rhs_hos tail, hosm_2d_par.c:181-233, and
-  // sol_update_RK bookkeeping, time_schemes_par.c:70-116)
+  // ---- RHS: end of an RK stage (rhs_hos tail, hosm_2d_par.c:181-233, and
+  // sol_update_RK bookkeeping, time_schemes_par.c:70-116).  blockIdx.y = 0
+  // finishes eta_t (and the Hamiltonian), blockIdx.y = 1 finishes phi_t.
+  __shared__ double red[MAX_THREADS / 32];
+  const int f = blockIdx.y;
   const int rows = a.rows_dev ? *a.rows_dev : a.rows;
   const bool live = row < rows;
   const bool fft_row = row < a.rows_fft;
   const size_t roff = (size_t)(live ? row : 0) * NX;
   const bool block_fft = (int)(blockIdx.x * lines) < a.rows_fft;
-  double2 se[E], sp[E];
+  C v[E];
   if (block_fft) {
-    const C* v0 = reinterpret_cast<const C*>(a.vin0);
-    const C* v1 = reinterpret_cast<const C*>(a.vin1);
-    C v[E];
+    const C* vin = reinterpret_cast<const C*>(f == 0 ? a.vin0 : a.vin1);
 #pragma unroll
-    for (int e = 0; e < E; e++) v[e] = fft_row ? v0[roff + t + e * P] : mkc((T)0, (T)0);
+    for (int e = 0; e < E; e++) v[e] = fft_row ? vin[roff + t + e * P] : mkc((T)0, (T)0);
     line_fft<T, NX, E, false>(v, sm, t, tw);
-#pragma unroll
-    for (int e = 0; e < E; e++) se[e] = widen(cscale(v[e], sc));
-#pragma unroll
-    for (int e = 0; e < E; e++) v[e] = fft_row ? v1[roff + t + e * P] : mkc((T)0, (T)0);
-    line_fft<T, NX, E, false>(v, sm, t, tw);
-#pragma unroll
-    for (int e = 0; e < E; e++) sp[e] = widen(cscale(v[e], sc));
   } else {
 #pragma unroll
-    for (int e = 0; e < E; e++) {
-      se[e] = make_double2(0.0, 0.0);
-      sp[e] = make_double2(0.0, 0.0);
-    }
+    for (int e = 0; e < E; e++) v[e] = mkc((T)0, (T)0);
   }
   double hacc = 0.0;
-  if (live) {
+  if (live && (fft_row || (f == 0 && a.ham))) {
     const double ky = ky_of(geo, row);
     const double R = *a.rdev;
     const double wrow = (row == 0) ? 1.0 : 2.0;  // Hamiltonian weights, hosm_2d_par.c:473-519
+    const size_t mine = f == 0 ? 0 : fsz, other = f == 0 ? fsz : 0;
 #pragma unroll
     for (int e = 0; e < E; e++) {
       const int i = t + e * P;
       const size_t idx = roff + i;
-      double2 ue = a.u[idx], up = a.u[fsz + idx];
-      const double2 u0e = ue, u0p = up;
+      const double2 u0 = a.u[mine + idx];  // this field at step start
+      double2 uo = a.u[other + idx];       // the other field's stage input
+      const double2 uo0 = uo;
       for (int p = 0; p < a.nk; p++) {
-        const double2 k0 = a.kp[p][idx], k1 = a.kp[p][fsz + idx];
-        ue.x = ue.x + a.coef[p] * k0.x;
-        ue.y = ue.y + a.coef[p] * k0.y;
-        up.x = up.x + a.coef[p] * k1.x;
-        up.y = up.y + a.coef[p] * k1.y;
+        const double2 k1 = a.kp[p][other + idx];
+        uo.x = uo.x + a.coef[p] * k1.x;
+        uo.y = uo.y + a.coef[p] * k1.y;
       }
-      double2 et = make_double2(0.0, 0.0), pt = make_double2(0.0, 0.0);
+      double2 kt = make_double2(0.0, 0.0);
       if (fft_row && keep_mode(geo, i, row)) {
-        const double kx = kx_of(geo, i);
-        const double kz = sqrt(kx * kx + ky * ky);
-        const double m1 = dz_mult(kz, geo.depth > 0 ? tanh(kz * geo.depth) : 1.0, 1);
-        // eta_t = R * NL_eta + Dz phi ; phi_t = R * NL_phi - g eta  (R = 1 without ramp)
-        et.x = R * se[e].x + m1 * up.x;
-        et.y = R * se[e].y + m1 * up.y;
-        pt.x = R * sp[e].x - geo.g * ue.x;
-        pt.y = R * sp[e].y - geo.g * ue.y;
+        const double2 s = cscale(widen(v[e]), geo.inv_nxny);
+        if (f == 0) {  // eta_t = R * NL_eta + Dz phi
+          const double kx = kx_of(geo, i);
+          const double m1 = dz_mult(geo, sqrt(kx * kx + ky * ky), 1);
+          kt.x = R * s.x + m1 * uo.x;
+          kt.y = R * s.y + m1 * uo.y;
+        } else {  // phi_t = R * NL_phi - g eta
+          kt.x = R * s.x - geo.g * uo.x;
+          kt.y = R * s.y - geo.g * uo.y;
+        }
       }
-      if (fft_row) {
-        a.kout[idx] = et;
-        a.kout[fsz + idx] = pt;
-      }
-      if (a.ham) {
-        hacc += wrow * (geo.g * u0e.x * u0e.x + geo.g * u0e.y * u0e.y + u0p.x * et.x + u0p.y * et.y);
-      }
+      if (fft_row) a.kout[mine + idx] = kt;
+      if (f == 0 && a.ham)  // g|eta|^2 + Re(phi conj(eta_t)) at step start (stage 0: stage input = u)
+        hacc += wrow * (geo.g * u0.x * u0.x + geo.g * u0.y * u0.y + uo0.x * kt.x + uo0.y * kt.y);
       if (a.final_update && fft_row) {
-        double2 ne = u0e, np = u0p;
+        double2 nu = u0;
         for (int s = 0; s + 1 < a.nstage; s++) {
-          const double2 k0 = a.kall[s][idx], k1 = a.kall[s][fsz + idx];
-          ne.x = ne.x + a.cfin[s] * k0.x;
-          ne.y = ne.y + a.cfin[s] * k0.y;
-          np.x = np.x + a.cfin[s] * k1.x;
-          np.y = np.y + a.cfin[s] * k1.y;
+          const double2 k0 = a.kall[s][mine + idx];
+          nu.x = nu.x + a.cfin[s] * k0.x;
+          nu.y = nu.y + a.cfin[s] * k0.y;
         }
         const double cl = a.cfin[a.nstage - 1];
-        ne.x = ne.x + cl * et.x;
-        ne.y = ne.y + cl * et.y;
-        np.x = np.x + cl * pt.x;
-        np.y = np.y + cl * pt.y;
-        a.unew[idx] = ne;
-        a.unew[fsz + idx] = np;
+        nu.x = nu.x + cl * kt.x;
+        nu.y = nu.y + cl * kt.y;
+        a.u[mine + idx] = nu;
       }
     }
   }
-  if (a.ham) {
+  if (f == 0 && a.ham) {
     // deterministic block reduction
-    for (int o = 16; o > 0; o >>= 1) hacc += __shfl_down_sync(0xffffffffu, hacc, o);
+    for (int off = 16; off > 0; off >>= 1) hacc += __shfl_down_sync(0xffffffffu, hacc, off);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = hacc;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -391,7 +316,13 @@ __global__ void __launch_bounds__(MAX_THREADS) k_xfwd(const __grid_constant__ XF
   }
 }
 
-// ---------------------------------------------------------------- y inverse
+// ---------------------------------------------------------------- y passes
+// Shared memory of a y-pass block: G line regions of `lp` complex elements.
+// A line region first holds the line's spectral column (index ky, padded by
+// spad) and then serves as the line FFT's exchange buffer.  lp >= h + h/E + 1
+// and lp is chosen so that the G-wide column strips move without bank
+// conflicts.
+
 struct YJob {
   int zin;  // input Z array index
   int iky;  // multiply by i*ky before the transform (Dy, operators_par.c:110)
@@ -400,16 +331,15 @@ struct YJob {
 
 struct YInvArgs {
   Geo geo;
-  int tp;            // tile pitch (complex elements per line)
+  int lp;            // line pitch in shared memory (complex elements)
   const void* z;     // Z arrays (T2), stride (h+1)*nx
   int rows_in;       // Z rows that may be nonzero; the rest are read as zero
   const int* rows_dev;  // if set, overrides rows_in
   void* phys;        // physical arrays (T), stride nx*ny
-  int njobs;
-  YJob jobs[MAX_JOBS];
-  // W_n epilogue on job 0 (hosm_2d_par.c:322-357 restated in physical space):
-  // W = job0 + sum_m phys[w_in[m]] * eta^w_pow[m] / w_pow[m]!
-  int wmode;
+  YJob jobs[MAX_JOBS];  // job of a block = jobs[blockIdx.y]
+  // LEVEL: the block of job 0 (order-1 derivative of phi^(n+1)) also forms
+  // W_n = job0 + sum_q phys[w_in[q]] * eta^w_pow[q] / w_pow[q]!
+  // (hosm_2d_par.c:322-357 restated in physical space)
   int w_out;
   int eta;
   int w_terms;
@@ -417,133 +347,128 @@ struct YInvArgs {
   int w_pow[MAX_TERMS];
 };
 
-template <typename T, int H, int E>
-__global__ void __launch_bounds__(MAX_THREADS) k_yinv(const __grid_constant__ YInvArgs a, const void* twv) {
+template <typename T, int H, int E, int MODE>
+__global__ void __launch_bounds__(MAX_THREADS, 2) k_yinv(const __grid_constant__ YInvArgs a, const void* twv,
+                                                         const void* twyv) {
   using C = cpx<T>;
   constexpr int P = H / E;
-  const C* tw = reinterpret_cast<const C*>(twv);
+  const C* tw = reinterpret_cast<const C*>(twv);    // length H
+  const C* twy = reinterpret_cast<const C*>(twyv);  // length 2H
   extern __shared__ __align__(16) unsigned char smraw[];
   const int G = blockDim.x / P;
   const int line = threadIdx.x / P;
   const int t = threadIdx.x - line * P;
-  C* tile = reinterpret_cast<C*>(smraw);
-  C* xb = tile + (size_t)G * a.tp + line * line_smem_elems<H, E>();
-  C* tl = tile + (size_t)line * a.tp;
+  C* sm = reinterpret_cast<C*>(smraw);
+  C* tl = sm + (size_t)line * a.lp;
   const Geo& geo = a.geo;
   const int nx = geo.nx;
+  const int ny = 2 * H;
   const int ix0 = blockIdx.x * G;
   const int ix = ix0 + line;
   const size_t fsz = (size_t)(H + 1) * nx;
-  const size_t psz = (size_t)nx * (2 * H);
-  const C* zall = reinterpret_cast<const C*>(a.z);
+  const size_t psz = (size_t)nx * ny;
+  const YJob J = a.jobs[blockIdx.y];
   T* pall = reinterpret_cast<T*>(a.phys);
-  const int ny = 2 * H;
-  const int tws = TW_N / ny;
 
-  int cur = -1;
-  for (int jb = 0; jb < a.njobs; jb++) {
-    const YJob J = a.jobs[jb];
-    if (J.zin != cur) {
-      __syncthreads();
-      const C* zs = zall + (size_t)J.zin * fsz;
-      const int nin = G * (a.rows_dev ? *a.rows_dev : a.rows_in);
-      const int ntot = G * (H + 1);
-      for (int q = threadIdx.x; q < ntot; q += blockDim.x) {
-        const int ky = q / G, g = q - ky * G;
-        tile[(size_t)g * a.tp + ky] = (q < nin) ? zs[(size_t)ky * nx + ix0 + g] : mkc((T)0, (T)0);
-      }
-      __syncthreads();
-      cur = J.zin;
+  {  // column strip -> line regions
+    const C* zs = reinterpret_cast<const C*>(a.z) + (size_t)J.zin * fsz;
+    const int nin = G * (a.rows_dev ? *a.rows_dev : a.rows_in);
+    const int ntot = G * (H + 1);
+    for (int q = threadIdx.x; q < ntot; q += blockDim.x) {
+      const int ky = q / G, g = q - ky * G;
+      sm[(size_t)g * a.lp + spad<E>(ky)] = (q < nin) ? zs[(size_t)ky * nx + ix0 + g] : mkc((T)0, (T)0);
     }
-    // complex-to-real preprocessing: c[k] = Xe + i Xo (packing of a length-Ny
-    // Hermitian sequence into a length-H complex one)
-    C v[E];
+  }
+  __syncthreads();
+  // complex-to-real preprocessing: c[k] = Xe + i Xo (packing of a length-Ny
+  // Hermitian sequence into a length-H complex one)
+  C v[E];
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    const int k = t + e * P;
+    C A = tl[spad<E>(k)];
+    C B = tl[spad<E>(H - k)];
+    if (J.iky) {
+      const T ka = (T)ky_of(geo, k), kb = (T)ky_of(geo, H - k);
+      A = cscale(cmul_i(A), ka);
+      B = cscale(cmul_i(B), kb);
+    }
+    if (k == 0) {  // FFTW c2r ignores Im of the ky = 0 and ky = Ny/2 bins
+      A.y = (T)0;
+      B.y = (T)0;
+    }
+    const C Bc = cconj(B);
+    const C xe = cadd(A, Bc);
+    const C d = csub(A, Bc);
+    const C w = cconj(__ldg(&twy[k]));  // exp(+2 pi i k / Ny)
+    v[e] = cadd(xe, cmul_i(cmul(d, w)));
+  }
+  line_fft<T, H, E, true>(v, tl, t, tw);  // starts with a barrier before reusing tl
+  // v[e] holds (x[2m], x[2m+1]) for m = t + e*P of physical row ix
+  C* po = reinterpret_cast<C*>(pall + (size_t)J.out * psz + (size_t)ix * ny);
+#pragma unroll
+  for (int e = 0; e < E; e++) po[t + e * P] = v[e];
+  if (MODE == YI_LEVEL && blockIdx.y == 0) {
+    const C* pe = reinterpret_cast<const C*>(pall + (size_t)a.eta * psz + (size_t)ix * ny);
+    C* pw = reinterpret_cast<C*>(pall + (size_t)a.w_out * psz + (size_t)ix * ny);
 #pragma unroll
     for (int e = 0; e < E; e++) {
-      const int k = t + e * P;
-      C A = tl[k];
-      C B = tl[H - k];
-      if (J.iky) {
-        const T ka = (T)ky_of(geo, k), kb = (T)ky_of(geo, H - k);
-        A = cscale(cmul_i(A), ka);
-        B = cscale(cmul_i(B), kb);
-      }
-      if (k == 0) {  // FFTW c2r ignores Im of the ky = 0 and ky = Ny/2 bins
-        A.y = (T)0;
-        B.y = (T)0;
-      }
-      const C Bc = cconj(B);
-      const C xe = cadd(A, Bc);
-      const C d = csub(A, Bc);
-      const C w = cconj(__ldg(&tw[k * tws]));  // exp(+2 pi i k / Ny)
-      const C xo = cmul(d, w);
-      v[e] = cadd(xe, cmul_i(xo));
-    }
-    line_fft<T, H, E, true>(v, xb, t, tw);
-    // v[e] holds (x[2m], x[2m+1]) for m = t + e*P of physical row ix
-    C* po = reinterpret_cast<C*>(pall + (size_t)J.out * psz + (size_t)ix * ny);
-#pragma unroll
-    for (int e = 0; e < E; e++) po[t + e * P] = v[e];
-    if (a.wmode && jb == 0) {
-      const C* pe = reinterpret_cast<const C*>(pall + (size_t)a.eta * psz + (size_t)ix * ny);
-      C* pw = reinterpret_cast<C*>(pall + (size_t)a.w_out * psz + (size_t)ix * ny);
-#pragma unroll
-      for (int e = 0; e < E; e++) {
-        const int m = t + e * P;
-        const C et = pe[m];
-        C acc = mkc((T)0, (T)0);
-        for (int q = 0; q < a.w_terms; q++) {
-          const C d = reinterpret_cast<const C*>(pall + (size_t)a.w_in[q] * psz + (size_t)ix * ny)[m];
-          T px = (T)1, py = (T)1, f = (T)1;
-          for (int r = 1; r <= a.w_pow[q]; r++) {
-            px *= et.x;
-            py *= et.y;
-            f *= (T)r;
-          }
-          acc.x += d.x * px / f;
-          acc.y += d.y * py / f;
+      const int m = t + e * P;
+      const C et = pe[m];
+      C acc = mkc((T)0, (T)0);
+      for (int q = 0; q < a.w_terms; q++) {
+        const C d = reinterpret_cast<const C*>(pall + (size_t)a.w_in[q] * psz + (size_t)ix * ny)[m];
+        T px = (T)1, py = (T)1, fct = (T)1;
+        for (int r = 1; r <= a.w_pow[q]; r++) {
+          px *= et.x;
+          py *= et.y;
+          fct *= (T)r;
         }
-        acc.x += v[e].x;
-        acc.y += v[e].y;
-        pw[m] = acc;
+        acc.x += d.x * px / fct;
+        acc.y += d.y * py / fct;
       }
+      acc.x += v[e].x;
+      acc.y += v[e].y;
+      pw[m] = acc;
     }
   }
 }
 
-// ---------------------------------------------------------------- y forward
 struct YFwdArgs {
   Geo geo;
-  int tp;
-  int mode;           // 0: plain (field in0); 1: Taylor level P_n; 2: RHS assembly (P_eta, P_phi)
+  int lp;
   const void* phys;   // physical arrays (T), stride nx*ny
-  const void* in_ptr; // mode 0: physical input (T) [nx][ny]
-  // mode 1: P = -sum_q phys[t_in[q]] * eta^t_pow[q] / t_pow[q]!  (hosm_2d_par.c:302-317)
+  const void* in_ptr; // PLAIN: physical input (T) [nx][ny]
+  // LEVEL: P = -sum_q phys[t_in[q]] * eta^t_pow[q] / t_pow[q]!  (hosm_2d_par.c:302-317)
   int eta;
   int nterms;
   int t_in[MAX_TERMS];
   int t_pow[MAX_TERMS];
-  // mode 2
+  // RHS (blockIdx.y = 0: P_eta, 1: P_phi)
   int ex, ey, px, py;
   int L;
   int w_idx[MAX_TERMS];  // W_0..W_L
-  void* vout;            // output V arrays (T2), stride (h+1)*nx
+  void* vout;            // output V arrays (T2), stride (h+1)*nx; output = blockIdx.y
   int rows_out;
 };
 
+// RHS assembly at one physical point: P_eta (which = 0) or P_phi (which = 1).
 template <typename T>
-__device__ __forceinline__ void rhs_point(const YFwdArgs& a, const T* const* Wp, size_t off, T ex, T ey, T px, T py,
-                                          T& pe, T& pp) {
+__device__ __forceinline__ T rhs_point(const YFwdArgs& a, const T* const* Wp, size_t off, T ex, T ey, T px, T py,
+                                       int which) {
   T W[MAX_TERMS];
   const int L = a.L;
 #pragma unroll
   for (int n = 0; n < MAX_TERMS; n++) W[n] = (n <= L) ? Wp[n][off] : (T)0;
   const T grad2 = ex * ex + ey * ey;
-  T s1 = (T)0, wm2 = (T)0;
+  if (which == 0) {
+    T s1 = (T)0, wm2 = (T)0;
 #pragma unroll
-  for (int n = 0; n < MAX_TERMS; n++) {
-    if (n >= 1 && n <= L) s1 += W[n];
-    if (n <= L - 2) wm2 += W[n];
+    for (int n = 0; n < MAX_TERMS; n++) {
+      if (n >= 1 && n <= L) s1 += W[n];
+      if (n <= L - 2) wm2 += W[n];
+    }
+    return -(ex * px + ey * py) + s1 + grad2 * wm2;  // hosm_2d_par.c:150-176
   }
   // W2M2 = sum_{n<=L-3} sum_m W_m W_{n-m};  W2M = W2M2 + sum_{n=L-2}^{L-1} ...  (hosm_2d_par.c:397-442)
   T w2m2 = (T)0, w2m = (T)0;
@@ -557,22 +482,22 @@ __device__ __forceinline__ void rhs_point(const YFwdArgs& a, const T* const* Wp,
     else w2m += s;
   }
   w2m += w2m2;
-  pe = -(ex * px + ey * py) + s1 + grad2 * wm2;                        // hosm_2d_par.c:150-176
-  pp = (T)0.5 * (w2m + grad2 * w2m2) - (T)0.5 * (px * px + py * py);  // hosm_2d_par.c:181-206
+  return (T)0.5 * (w2m + grad2 * w2m2) - (T)0.5 * (px * px + py * py);  // hosm_2d_par.c:181-206
 }
 
-template <typename T, int H, int E>
-__global__ void __launch_bounds__(MAX_THREADS) k_yfwd(const __grid_constant__ YFwdArgs a, const void* twv) {
+template <typename T, int H, int E, int MODE>
+__global__ void __launch_bounds__(MAX_THREADS, 2) k_yfwd(const __grid_constant__ YFwdArgs a, const void* twv,
+                                                         const void* twyv) {
   using C = cpx<T>;
   constexpr int P = H / E;
   const C* tw = reinterpret_cast<const C*>(twv);
+  const C* twy = reinterpret_cast<const C*>(twyv);
   extern __shared__ __align__(16) unsigned char smraw[];
   const int G = blockDim.x / P;
   const int line = threadIdx.x / P;
   const int t = threadIdx.x - line * P;
-  C* tile = reinterpret_cast<C*>(smraw);
-  C* xb = tile + (size_t)G * a.tp + line * line_smem_elems<H, E>();
-  C* tl = tile + (size_t)line * a.tp;
+  C* sm = reinterpret_cast<C*>(smraw);
+  C* tl = sm + (size_t)line * a.lp;
   const Geo& geo = a.geo;
   const int nx = geo.nx;
   const int ny = 2 * H;
@@ -582,16 +507,13 @@ __global__ void __launch_bounds__(MAX_THREADS) k_yfwd(const __grid_constant__ YF
   const size_t psz = (size_t)nx * ny;
   const T* pall = reinterpret_cast<const T*>(a.phys);
   const size_t rowoff = (size_t)ix * ny;
-  C* vall = reinterpret_cast<C*>(a.vout);
-  const int tws = TW_N / ny;
-  const int nout = (a.mode == 2) ? 2 : 1;
 
-  C v[E], v2[E];
-  if (a.mode == 0) {
+  C v[E];
+  if (MODE == YF_PLAIN) {
     const C* src = reinterpret_cast<const C*>(reinterpret_cast<const T*>(a.in_ptr) + rowoff);
 #pragma unroll
     for (int e = 0; e < E; e++) v[e] = src[t + e * P];
-  } else if (a.mode == 1) {
+  } else if (MODE == YF_LEVEL) {
     const C* pe = reinterpret_cast<const C*>(pall + (size_t)a.eta * psz + rowoff);
 #pragma unroll
     for (int e = 0; e < E; e++) {
@@ -600,18 +522,19 @@ __global__ void __launch_bounds__(MAX_THREADS) k_yfwd(const __grid_constant__ YF
       C acc = mkc((T)0, (T)0);
       for (int q = 0; q < a.nterms; q++) {
         const C d = reinterpret_cast<const C*>(pall + (size_t)a.t_in[q] * psz + rowoff)[m];
-        T px = (T)1, py = (T)1, f = (T)1;
+        T px = (T)1, py = (T)1, fct = (T)1;
         for (int r = 1; r <= a.t_pow[q]; r++) {
           px *= et.x;
           py *= et.y;
-          f *= (T)r;
+          fct *= (T)r;
         }
-        acc.x -= d.x * px / f;
-        acc.y -= d.y * py / f;
+        acc.x -= d.x * px / fct;
+        acc.y -= d.y * py / fct;
       }
       v[e] = acc;
     }
   } else {
+    const int which = blockIdx.y;
     const T* Wp[MAX_TERMS];
 #pragma unroll
     for (int n = 0; n < MAX_TERMS; n++) Wp[n] = pall + (size_t)a.w_idx[n < a.L + 1 ? n : 0] * psz + rowoff;
@@ -622,46 +545,49 @@ __global__ void __launch_bounds__(MAX_THREADS) k_yfwd(const __grid_constant__ YF
 #pragma unroll
     for (int e = 0; e < E; e++) {
       const int m = t + e * P;
-      T pe0, pp0, pe1, pp1;
-      rhs_point<T>(a, Wp, 2 * m, pex[2 * m], pey[2 * m], ppx[2 * m], ppy[2 * m], pe0, pp0);
-      rhs_point<T>(a, Wp, 2 * m + 1, pex[2 * m + 1], pey[2 * m + 1], ppx[2 * m + 1], ppy[2 * m + 1], pe1, pp1);
-      v[e] = mkc(pe0, pe1);
-      v2[e] = mkc(pp0, pp1);
+      const T r0 = rhs_point<T>(a, Wp, 2 * m, pex[2 * m], pey[2 * m], ppx[2 * m], ppy[2 * m], which);
+      const T r1 = rhs_point<T>(a, Wp, 2 * m + 1, pex[2 * m + 1], pey[2 * m + 1], ppx[2 * m + 1], ppy[2 * m + 1], which);
+      v[e] = mkc(r0, r1);
     }
   }
 
-  for (int o = 0; o < nout; o++) {
-    if (o == 1) {
+  line_fft<T, H, E, false>(v, tl, t, tw);
+  // C[k] natural order -> line region, then real-to-complex postprocessing in
+  // place, one (k, H-k) pair per thread slot
+  __syncthreads();
 #pragma unroll
-      for (int e = 0; e < E; e++) v[e] = v2[e];
-    }
-    line_fft<T, H, E, false>(v, xb, t, tw);
-    // C[k] natural order -> shared buffer, then real-to-complex postprocessing
-    __syncthreads();
+  for (int e = 0; e < E; e++) tl[spad<E>(t + e * P)] = v[e];
+  __syncthreads();
 #pragma unroll
-    for (int e = 0; e < E; e++) xb[spad<E>(t + e * P)] = v[e];
-    __syncthreads();
-#pragma unroll
-    for (int e = 0; e <= E; e++) {
-      int k;
-      if (e < E) k = t + e * P;
-      else if (t == 0) k = H;
-      else break;
-      const C ck = xb[spad<E>(k & (H - 1))];
-      const C cn = cconj(xb[spad<E>((H - k) & (H - 1))]);
-      const C ev = cscale(cadd(ck, cn), (T)0.5);
-      const C d = csub(ck, cn);
-      const C od = mkc((T)0.5 * d.y, (T)-0.5 * d.x);  // (ck - cn) / (2i)
-      const C w = __ldg(&tw[k * tws]);              // exp(-2 pi i k / Ny)
-      tl[k] = cadd(ev, cmul(w, od));
+  for (int e = 0; e <= E / 2; e++) {
+    int k;
+    if (e < E / 2) k = t + e * P;  // pairs (k, H-k), k in [0, H/2)
+    else if (t == 0) k = H / 2;    // the self-paired middle bin
+    else break;
+    const int kn = H - k;  // partner; for k = 0 the partner is the Nyquist bin H (C[H] = C[0])
+    const C ck = tl[spad<E>(k)];
+    const C cq = tl[spad<E>(kn & (H - 1))];
+    // X[k] = (C[k] + conj C[H-k])/2 + w^k (C[k] - conj C[H-k])/(2i),  w = exp(-2 pi i / Ny)
+    const C cn = cconj(cq);
+    const C ev = cscale(cadd(ck, cn), (T)0.5);
+    const C d = csub(ck, cn);
+    const C od = mkc((T)0.5 * d.y, (T)-0.5 * d.x);
+    const C xk = cadd(ev, cmul(__ldg(&twy[k]), od));
+    if (k != kn) {
+      const C cm = cconj(ck);
+      const C ev2 = cscale(cadd(cq, cm), (T)0.5);
+      const C d2 = csub(cq, cm);
+      const C od2 = mkc((T)0.5 * d2.y, (T)-0.5 * d2.x);
+      tl[spad<E>(kn)] = cadd(ev2, cmul(__ldg(&twy[kn]), od2));
     }
-    __syncthreads();
-    C* vo = vall + (size_t)o * fsz;
-    const int ntot = G * a.rows_out;
-    for (int q = threadIdx.x; q < ntot; q += blockDim.x) {
-      const int ky = q / G, g = q - ky * G;
-      vo[(size_t)ky * nx + ix0 + g] = tile[(size_t)g * a.tp + ky];
-    }
+    tl[spad<E>(k)] = xk;
+  }
+  __syncthreads();
+  C* vo = reinterpret_cast<C*>(a.vout) + (size_t)blockIdx.y * fsz;
+  const int ntot = G * a.rows_out;
+  for (int q = threadIdx.x; q < ntot; q += blockDim.x) {
+    const int ky = q / G, g = q - ky * G;
+    vo[(size_t)ky * nx + ix0 + g] = sm[(size_t)g * a.lp + spad<E>(ky)];
   }
 }
 

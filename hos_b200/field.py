@@ -190,6 +190,26 @@ class HosField:
         _lib.check(self._lib.hos_check_finite(self._h, ctypes.byref(f)))
         return bool(f.value)
 
+    def profile_stage(self, dt, reps=5):
+        """Per-pass timing of one RK stage: list of dicts with name,
+        launches_per_stage, ms_per_launch, bytes_per_launch."""
+        arr = (_lib.HosPassStat * 16)()
+        n = ctypes.c_int()
+        _lib.check(self._lib.hos_profile_stage(self._h, float(dt), int(reps), arr, 16, ctypes.byref(n)))
+        return [
+            {
+                "name": arr[i].name.decode(),
+                "launches_per_stage": arr[i].launches_per_stage,
+                "ms_per_launch": arr[i].ms_per_launch,
+                "bytes_per_launch": arr[i].bytes_per_launch,
+            }
+            for i in range(n.value)
+        ]
+
+    @property
+    def launches_per_step(self):
+        return int(self._lib.hos_launches_per_step(self._h))
+
     def volume(self):
         v = ctypes.c_double()
         _lib.check(self._lib.hos_volume(self._h, ctypes.byref(v)))

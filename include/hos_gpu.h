@@ -121,6 +121,22 @@ int hos_check_finite(hos_handle h, int* finite);
 /* Volume (the k = 0 mode of eta_hat, real part) of the resident state. */
 int hos_volume(hos_handle h, double* vol);
 
+/* Per-pass timing of one RK stage on the resident state (written to
+ * scratch; the state is untouched).  Each pass kind gets one record: the
+ * number of its launches in a stage, the mean duration of a launch (CUDA
+ * events on the handle's stream, averaged over reps) and the algorithmic
+ * bytes of a launch (what the pass must read plus write). */
+typedef struct hos_pass_stat {
+  char name[32];
+  int launches_per_stage;
+  double ms_per_launch;
+  double bytes_per_launch;
+} hos_pass_stat;
+int hos_profile_stage(hos_handle h, double dt, int reps, hos_pass_stat* out, int max, int* count);
+
+/* Kernel launches of this library in one RK step of the handle. */
+int hos_launches_per_step(hos_handle h);
+
 /* CUDA stream of the handle (a cudaStream_t), for callers that order their
  * own work against it. */
 void* hos_stream(hos_handle h);
