@@ -1,0 +1,449 @@
+#!/usr/bin/env python
+"""Benchmark of the HOS time advance on B200: RK4 steps/s at 1024^2, M = 5.
+
+Workload (the precision-form configuration): a directional JONSWAP sea on a
+2 pi x 2 pi doubly periodic domain, Nx = Ny = 1024, HOS order M = 5, peak
+wavenumber kp = 24, kp*Hs/2 = 0.12, gamma = 3.3, cos^(2s)(theta/2) spreading
+with s = 10, seeded complex-Gaussian mode amplitudes, linear phi_s, g = 1,
+deep water, RK4 with dt = Tp/50.  Synthetic data (seeded); the reference
+ships no benchmark inputs.
+
+One bench step = one RK4 step of that field.  ``value`` is the FP32-compute
+form (FP32 transforms/products/RHS, FP64 RK state and diagnostics); the FP64
+drop-in path is timed beside it, and both are run on to 1000 steps to report
+the FP32 form's eta error relative to Hs.  Inputs are resident in HBM when
+the timed region starts; the per-step working set (about 230 MB in FP32,
+400 MB in FP64) exceeds the 126 MB L2, so no explicit flush is used.
+
+``e2e`` is the same metric through the C ABI with host buffers: every step
+uploads the packed spectral state from pinned host memory, advances one RK4
+step and reads the state back.
+
+With --gpus N (torchrun, one rank per GPU) every rank advances its own
+independent field (replicas: the path does not shard); ``value`` counts the
+steps of all ranks over the slowest rank's time.
+
+--impl reference times the reference's own CPU implementation of the path
+(the Csource/2dpar hot-path sources built with the single-rank FFTW-MPI shim,
+oracle/_ref) on the same workload and prints the same JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RK4 steps/s at 1024^2 M=5, FP32 vs FP64 (eta err<=1e-5); ensemble p50/p99 latency"
+UNIT = "RK4 steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=1024)
+    ap.add_argument("--order", type=int, default=5)
+    ap.add_argument("--accuracy-steps", type=int, default=1000)
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(n, order, seed):
+    from hos_b200 import ic
+
+    eta, phi, info = ic.jonswap(n, n, kp=24.0 * n / 1024, steepness=0.12, gamma=3.3, spread_s=10.0, seed=seed)
+    dt = info["Tp"] / 50
+    desc = (f"{n}x{n} M={order} JONSWAP kp={24.0 * n / 1024:g} kp*Hs/2=0.12 gamma=3.3 s=10 deep water, "
+            f"RK4 dt=Tp/50, 2pi domain, g=1")
+    return eta, phi, info, dt, desc
+
+
+def config(args, desc):
+    return {
+        "workload": desc,
+        "n": args.n,
+        "order": args.order,
+        "scheme": "RK4",
+        "state": "FP64 spectral, resident in HBM",
+        "l2": "per-step working set > 126 MB L2 (no flush)",
+        "parallelism": f"replicas x{args.gpus}" if args.gpus > 1 else "single GPU",
+    }
+
+
+# ------------------------------------------------------------------ clocks
+class Clocks:
+    """nvidia-smi sampled every 200 ms while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.path)
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": max(smax) if smax else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+# ------------------------------------------------------------------ helpers
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the pass kinds from the committed ncu summary
+    (profiles/ncu_traffic.txt: lines '<pass> <precision> <n> <bytes>')."""
+    out = {}
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    if os.path.exists(path):
+        for line in open(path):
+            f = line.split()
+            if len(f) == 4 and not line.startswith("#"):
+                out[(f[0], f[1], int(f[2]))] = float(f[3])
+    return out
+
+
+def algorithmic_step_bytes(n, order, prec_bytes):
+    """Survey byte model per RK4 step: 4*T_M*(R_p + C_p) + 26*C_64."""
+    tm = 6 + order + order * (order + 1) // 2
+    R = n * n * prec_bytes
+    C = n * (n // 2 + 1) * 2 * prec_bytes
+    C64 = n * (n // 2 + 1) * 16
+    return 4 * tm * (R + C) + 26 * C64
+
+
+def cpu_reference_rate(args, eta, phi, info, dt, max_seconds):
+    """The reference's own hot path (oracle/_ref, all host threads) on the
+    workload: RK4 steps/s over a bounded number of steps."""
+    from oracle import ref_c
+
+    if not ref_c.available(args.order):
+        return None
+    ref = ref_c.RefC(args.order, args.n, args.n, g=1.0, scheme=2)
+    u = ref.init_state(eta, phi)
+    t0 = time.perf_counter()
+    u, t, _ = ref.steps(u, 0.0, dt, 1)
+    first = time.perf_counter() - t0
+    nsteps = max(1, min(20, int(max_seconds / max(first, 1e-9))))
+    t0 = time.perf_counter()
+    u, t, _ = ref.steps(u, t, dt, nsteps)
+    el = time.perf_counter() - t0
+    return {"value": nsteps / el, "steps": nsteps, "seconds": el}
+
+
+# ------------------------------------------------------------------ reference arm
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    cores = int(os.environ["OMP_NUM_THREADS"])
+    eta, phi, info, dt, desc = workload(args.n, args.order, seed=1000)
+    from oracle import ref_c
+
+    if not ref_c.available(args.order):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (make -C oracle)"}))
+        return
+    ref = ref_c.RefC(args.order, args.n, args.n, g=1.0, scheme=2)
+    u = ref.init_state(eta, phi)
+    t = 0.0
+    # bounded: warm-up and timed counts are clipped so the run ends in a few minutes
+    t0 = time.perf_counter()
+    u, t, _ = ref.steps(u, t, dt, 1)
+    per = time.perf_counter() - t0
+    budget = 150.0
+    warm = max(0, min(args.warmup - 1, int(0.2 * budget / per)))
+    if warm:
+        u, t, _ = ref.steps(u, t, dt, warm)
+    k = max(1, min(args.steps, int(0.8 * budget / per)))
+    t0 = time.perf_counter()
+    u, t, _ = ref.steps(u, t, dt, k)
+    el = time.perf_counter() - t0
+    v = k / el
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": v,
+        "unit": UNIT,
+        "n_gpus": args.gpus,
+        "steps": k,
+        "warmup": warm + 1,
+        "ms_per_step": 1e3 * el / k,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded JONSWAP)",
+        "config": config(args, desc),
+        "cpu_baseline": {
+            "value": v,
+            "unit": UNIT,
+            "cores": cores,
+            "kind": "reference",
+            "sample": f"{k} RK4 steps of the {args.n}^2 M={args.order} field after {warm + 1} warm-up steps "
+                      "(Csource/2dpar hot-path sources, single-rank FFTW-MPI shim, OpenMP FFT lines)",
+        },
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "gpu_launches": 0,
+    }
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args, rank, world, local_rank):
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from hos_b200 import HosField
+
+    torch.cuda.set_device(local_rank)
+    dist = world > 1
+    if dist:
+        import torch.distributed as tdist
+
+    def barrier():
+        if dist:
+            tdist.barrier()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        return float(t.item())
+
+    eta, phi, info, dt, desc = workload(args.n, args.order, seed=1000 + rank)
+    fields = {p: HosField(args.n, args.n, order=args.order, precision=p) for p in ("fp64", "fp32")}
+    for f in fields.values():
+        f.set_state_physical(eta, phi)
+    clocks = Clocks(local_rank)
+    timings = {}
+    clocks.start()
+    for p in ("fp64", "fp32"):
+        f = fields[p]
+        stream = torch.cuda.ExternalStream(f.stream)
+        f.step(dt, args.warmup)
+        f.sync()
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        f.step(dt, args.steps)
+        e1.record(stream)
+        f.sync()
+        torch.cuda.synchronize()
+        barrier()
+        timings[p] = max_over_ranks(e0.elapsed_time(e1))
+    clk = clocks.stop()
+    steps_done = args.warmup + args.steps
+    v64 = world * args.steps / (timings["fp64"] / 1e3)
+    v32 = world * args.steps / (timings["fp32"] / 1e3)
+
+    # per-pass live timing of the FP32 form -> dominant kernel roofline
+    passes = fields["fp32"].profile_stage(dt, reps=5)
+    dom = max(passes, key=lambda d: d["launches_per_stage"] * d["ms_per_launch"])
+    peak, peak_kind = peaks()
+    achieved = dom["bytes_per_launch"] / (dom["ms_per_launch"] * 1e-3) / 1e9
+    traffic = ncu_traffic().get((dom["name"], "fp32", args.n))
+    stage_ms = sum(d["launches_per_stage"] * d["ms_per_launch"] for d in passes)
+
+    # accuracy: both forms on to accuracy_steps, eta error relative to Hs
+    for f in fields.values():
+        if args.accuracy_steps > steps_done:
+            f.step(dt, args.accuracy_steps - steps_done)
+        f.sync()
+    e64, p64 = fields["fp64"].state_physical()
+    e32, p32 = fields["fp32"].state_physical()
+    _, H64 = fields["fp64"].energy_history()
+    _, H32 = fields["fp32"].energy_history()
+    eta_err = float(np.max(np.abs(e32 - e64)) / info["Hs"])
+    phi_err = float(np.max(np.abs(p32 - p64)) / np.max(np.abs(p64)))
+    ham_err = float(np.max(np.abs(H32 - H64)) / np.max(np.abs(H64)))
+    energy_drift = float(abs(H64[-1] - H64[0]) / abs(H64[0]))
+    nsteps_acc = max(args.accuracy_steps, steps_done)
+
+    # e2e through the C ABI with pinned host buffers
+    f = fields["fp32"]
+    u0, _ = f.state_spectral()
+    host = torch.empty((2, args.n // 2 + 1, args.n), dtype=torch.complex128, pin_memory=True)
+    hnp = host.numpy()
+    hnp[...] = u0
+    stream = torch.cuda.ExternalStream(f.stream)
+    for _ in range(2):
+        f.set_state_spectral(hnp)
+        f.step(dt, 1)
+        st = f.state_spectral()  # noqa: F841 (warm-up of the path)
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    hp = ctypes.c_void_p(hnp.ctypes.data)
+    rcs = 0
+    for _ in range(args.e2e_steps):
+        rcs |= f._lib.hos_set_state_spectral(f._h, hp, 0.0)
+        rcs |= f._lib.hos_step(f._h, dt, 1)
+        rcs |= f._lib.hos_get_state_spectral(f._h, hp, None)
+    e1.record(stream)
+    if rcs:
+        raise RuntimeError("e2e path returned an error")
+    f.sync()
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    state_bytes = 2 * (args.n // 2 + 1) * args.n * 16
+
+    line = {
+        "metric": METRIC,
+        "value": v32,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": timings["fp32"] / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 compute, f64 state",
+        "data": "synthetic (seeded JONSWAP)",
+        "config": config(args, desc),
+        "fp64": {"value": v64, "ms_per_step": timings["fp64"] / args.steps},
+        "fp32_over_fp64": v32 / v64,
+        "accuracy": {
+            "steps": nsteps_acc,
+            "eta_err_over_Hs": eta_err,
+            "phi_err_rel": phi_err,
+            "energy_err_rel": ham_err,
+            "fp64_energy_drift_rel": energy_drift,
+            "target_eta_err_over_Hs": 1e-5,
+        },
+        "roofline": {
+            "bound": "hbm",
+            "kernel": dom["name"],
+            "achieved": achieved,
+            "peak": peak,
+            "peak_kind": f"{peak_kind} copy bandwidth (burst)",
+            "unit": "GB/s",
+            "frac": achieved / peak,
+            "traffic": traffic,
+            "bytes_per_launch": dom["bytes_per_launch"],
+            "ms_per_launch": dom["ms_per_launch"],
+            "share_of_stage": dom["launches_per_stage"] * dom["ms_per_launch"] / stage_ms,
+        },
+        "passes": passes,
+        "step_roofline": {
+            "model_bytes_per_step": algorithmic_step_bytes(args.n, args.order, 4),
+            "achieved_gbs": algorithmic_step_bytes(args.n, args.order, 4) / (timings["fp32"] / args.steps * 1e-3) / 1e9,
+            "peak": peak,
+        },
+        "e2e": {
+            "value": world * args.e2e_steps / (e2e_ms / 1e3),
+            "unit": UNIT,
+            "h2d_bytes_per_step": state_bytes + 8,
+            "d2h_bytes_per_step": state_bytes + 8,
+            "path": "hos_set_state_spectral (pinned host) + hos_step + hos_get_state_spectral",
+        },
+        "gpu_launches": args.steps * f.launches_per_step,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+        cb = cpu_reference_rate(args, eta, phi, info, dt, max_seconds=20.0)
+        if cb is not None:
+            line["cpu_baseline"] = {
+                "value": cb["value"],
+                "unit": UNIT,
+                "cores": int(os.environ["OMP_NUM_THREADS"]),
+                "kind": "reference",
+                "sample": f"{cb['steps']} RK4 steps ({cb['seconds']:.1f} s) of the same field on the host "
+                          "(Csource/2dpar hot-path sources with the single-rank FFTW-MPI shim)",
+            }
+    for fl in fields.values():
+        fl.close()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as tdist
+
+            tdist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

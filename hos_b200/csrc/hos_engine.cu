@@ -247,6 +247,7 @@ struct hos_ctx {
   void* zbuf = nullptr;
   void* phys = nullptr;
   double2* ustage = nullptr;
+  double2* ustg = nullptr;  // stage input of the current RK stage
   double2* zplain = nullptr;
   double* pplain = nullptr;
   void* tw[2][3] = {};  // [precision][nx, ny/2, ny] twiddle tables
@@ -348,6 +349,7 @@ size_t compute_bytes(const hos_params* p, int nst) {
   b += (size_t)(4 + M) * fsz * cs;                   // Z / V scratch
   b += (size_t)(5 + M * (M + 1) / 2 + L) * psz * rs; // physical fields
   b += 2 * fsz * 16 + fsz * 16 + 2 * psz * 8;        // boundary scratch (FP64)
+  b += 2 * fsz * 16;                                 // stage input
   b += (nx + h + ny) * (16 + 8);
   b += 2 * (size_t)HIST_CAP * 8 + 4096 * 8 + 4096;
   return b;
@@ -407,6 +409,7 @@ int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, dou
   }
   xa.nk = nk;
   xa.z = c->zbuf;
+  xa.ustg = c->ustg;
   xa.tdev = tsrc;
   xa.rdev = c->rdev;
   xa.set_ramp = (s == 0);
@@ -499,11 +502,7 @@ int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, dou
   xe.vin0 = zb;
   xe.vin1 = zb + fsz * cs;
   xe.u = uin;
-  for (int p = 0; p < nk; p++) {
-    xe.kp[p] = xa.kp[p];
-    xe.coef[p] = xa.coef[p];
-  }
-  xe.nk = nk;
+  xe.ustg = c->ustg;
   xe.kout = kout;
   xe.rdev = c->rdev;
   xe.ham = (!rhs_only && s == 0);
@@ -612,7 +611,7 @@ void release(hos_ctx* c) {
   if (!c) return;
   if (c->gexec) cudaGraphExecDestroy(c->gexec);
   if (c->graph) cudaGraphDestroy(c->graph);
-  void* ptrs[] = {c->u,    c->k,    c->zbuf,    c->phys,   c->ustage, c->zplain,   c->pplain,
+  void* ptrs[] = {c->u,    c->k,    c->zbuf,    c->phys,   c->ustage, c->ustg, c->zplain,   c->pplain,
                   c->tdev, c->trhs, c->rdev,    c->stepdev, c->actdev, c->flagdev, c->ham_part,
                   c->ham_hist, c->t_hist, c->tw[0][0], c->tw[0][1], c->tw[0][2], c->tw[1][0], c->tw[1][1], c->tw[1][2]};
   for (void* p : ptrs)
@@ -731,6 +730,7 @@ int hos_create(const hos_params* p, hos_handle* out) {
   HOS_AL(c->zbuf, (size_t)c->nz * c->fsz * cs);
   HOS_AL(c->phys, (size_t)c->nphys * c->psz * rs);
   HOS_AL(c->ustage, 2 * c->fsz * sizeof(double2));
+  HOS_AL(c->ustg, 2 * c->fsz * sizeof(double2));
   HOS_AL(c->zplain, c->fsz * sizeof(double2));
   HOS_AL(c->pplain, 2 * c->psz * sizeof(double));
   {

@@ -77,6 +77,7 @@ struct XInvArgs {
   double coef[MAX_STAGES];        // dt*b[s][p]
   int nk;
   void* z;              // output complex arrays (T2), stride (h+1)*nx; output o = blockIdx.y
+  double2* ustg;        // STAGE: the stage input is also stored here ([2][h+1][nx], rows < rows)
   const double* tdev;   // simulation time (device)
   double* rdev;         // ramp factor for this step (device), written if set_ramp
   int set_ramp;
@@ -136,6 +137,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_xinv(const __grid_constant__
           x.y = x.y + a.coef[p] * kk.y;
         }
       }
+      if ((o == 0 || o == 2) && live) a.ustg[foff + roff + i] = x;
       if (o == 1 || o == 3) {  // Dx: i kx (operators_par.c:66)
         const double kx = kx_of(geo, i);
         x = make_double2(-kx * x.y, kx * x.x);
@@ -168,9 +170,9 @@ struct XFwdArgs {
   int ndz;              // LEVEL: z-derivative orders 1..ndz
   // RHS
   double2* u;                     // packed state at step start (updated in place on the final stage)
-  const double2* kp[MAX_STAGES];  // earlier stage derivatives (stage input = u + sum coef*kp)
-  double coef[MAX_STAGES];
-  int nk;
+  const double2* ustg;            // stage input of both fields, written by the x-inverse pass
+                                  // (never read from u: on the final stage the other field's
+                                  // blocks overwrite u)
   double2* kout;                  // this stage's derivative [2][h+1][nx]
   const double* rdev;             // ramp factor
   int ham;                        // accumulate the stage-0 Hamiltonian
@@ -265,14 +267,8 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_xfwd(const __grid_constant__
     for (int e = 0; e < E; e++) {
       const int i = t + e * P;
       const size_t idx = roff + i;
-      const double2 u0 = a.u[mine + idx];  // this field at step start
-      double2 uo = a.u[other + idx];       // the other field's stage input
-      const double2 uo0 = uo;
-      for (int p = 0; p < a.nk; p++) {
-        const double2 k1 = a.kp[p][other + idx];
-        uo.x = uo.x + a.coef[p] * k1.x;
-        uo.y = uo.y + a.coef[p] * k1.y;
-      }
+      const double2 u0 = a.u[mine + idx];   // this field at step start
+      const double2 uo = a.ustg[other + idx];  // the other field's stage input (= u at stage 0)
       double2 kt = make_double2(0.0, 0.0);
       if (fft_row && keep_mode(geo, i, row)) {
         const double2 s = cscale(widen(v[e]), geo.inv_nxny);
@@ -288,7 +284,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_xfwd(const __grid_constant__
       }
       if (fft_row) a.kout[mine + idx] = kt;
       if (f == 0 && a.ham)  // g|eta|^2 + Re(phi conj(eta_t)) at step start (stage 0: stage input = u)
-        hacc += wrow * (geo.g * u0.x * u0.x + geo.g * u0.y * u0.y + uo0.x * kt.x + uo0.y * kt.y);
+        hacc += wrow * (geo.g * u0.x * u0.x + geo.g * u0.y * u0.y + uo.x * kt.x + uo.y * kt.y);
       if (a.final_update && fft_row) {
         double2 nu = u0;
         for (int s = 0; s + 1 < a.nstage; s++) {
