@@ -108,48 +108,64 @@ __device__ __forceinline__ float2 conv<float>(double2 a) {
 __device__ __forceinline__ double2 widen(double2 a) { return a; }
 __device__ __forceinline__ double2 widen(float2 a) { return to_d(a); }
 
-// cos(2 pi m / 16), m = 0..15, correctly rounded decimal literals.
-__device__ __forceinline__ double cos16(int m) {
-  switch (m & 15) {
+// cos(2 pi m / 32), m = 0..31, correctly rounded decimal literals.
+__device__ __forceinline__ double cos32(int m) {
+  switch (m & 31) {
     case 0: return 1.0;
-    case 1: return 0.92387953251128675613;
-    case 2: return 0.70710678118654752440;
-    case 3: return 0.38268343236508977173;
-    case 4: return 0.0;
-    case 5: return -0.38268343236508977173;
-    case 6: return -0.70710678118654752440;
-    case 7: return -0.92387953251128675613;
-    case 8: return -1.0;
-    case 9: return -0.92387953251128675613;
-    case 10: return -0.70710678118654752440;
-    case 11: return -0.38268343236508977173;
-    case 12: return 0.0;
-    case 13: return 0.38268343236508977173;
-    case 14: return 0.70710678118654752440;
-    default: return 0.92387953251128675613;
+    case 1: return 0.98078528040323044913;
+    case 2: return 0.92387953251128675613;
+    case 3: return 0.83146961230254523708;
+    case 4: return 0.70710678118654752440;
+    case 5: return 0.55557023301960222474;
+    case 6: return 0.38268343236508977173;
+    case 7: return 0.19509032201612826785;
+    case 8: return 0.0;
+    case 9: return -0.19509032201612826785;
+    case 10: return -0.38268343236508977173;
+    case 11: return -0.55557023301960222474;
+    case 12: return -0.70710678118654752440;
+    case 13: return -0.83146961230254523708;
+    case 14: return -0.92387953251128675613;
+    case 15: return -0.98078528040323044913;
+    case 16: return -1.0;
+    case 17: return -0.98078528040323044913;
+    case 18: return -0.92387953251128675613;
+    case 19: return -0.83146961230254523708;
+    case 20: return -0.70710678118654752440;
+    case 21: return -0.55557023301960222474;
+    case 22: return -0.38268343236508977173;
+    case 23: return -0.19509032201612826785;
+    case 24: return 0.0;
+    case 25: return 0.19509032201612826785;
+    case 26: return 0.38268343236508977173;
+    case 27: return 0.55557023301960222474;
+    case 28: return 0.70710678118654752440;
+    case 29: return 0.83146961230254523708;
+    case 30: return 0.92387953251128675613;
+    default: return 0.98078528040323044913;
   }
 }
 
-// b * exp(sgn * 2 pi i m / R) with R <= 16, m compile-time after unrolling.
+// b * exp(sgn * 2 pi i m / R) with R <= 32, m compile-time after unrolling.
 template <int R, bool INV, typename C>
 __device__ __forceinline__ C twc(C b, int m) {
-  const int m16 = (m * (16 / R)) & 15;
-  if (m16 == 0) return b;
-  if (m16 == 4) {  // forward: times -i, inverse: times +i
+  const int m32 = (m * (32 / R)) & 31;
+  if (m32 == 0) return b;
+  if (m32 == 8) {  // forward: times -i, inverse: times +i
     C r;
     r.x = INV ? -b.y : b.y;
     r.y = INV ? b.x : -b.x;
     return r;
   }
-  if (m16 == 8) {
+  if (m32 == 16) {
     C r;
     r.x = -b.x;
     r.y = -b.y;
     return r;
   }
   using S = decltype(b.x);
-  S c = (S)cos16(m16);
-  S s = (S)cos16(m16 - 4);  // sin(2 pi m16/16)
+  S c = (S)cos32(m32);
+  S s = (S)cos32(m32 - 8);  // sin(2 pi m32/32)
   if (!INV) s = -s;
   C w;
   w.x = c;
@@ -157,7 +173,7 @@ __device__ __forceinline__ C twc(C b, int m) {
   return cmul(b, w);
 }
 
-// In-register R-point DFT (R in {2,4,8,16}), natural order in and out,
+// In-register R-point DFT (R in {2,4,8,16,32}), natural order in and out,
 // forward exp(-i...), inverse exp(+i...), unnormalised.
 template <int R>
 __device__ __forceinline__ constexpr int bitrev(int i) {
@@ -196,15 +212,24 @@ __device__ __forceinline__ constexpr int ilog2c() {
   return r;
 }
 
-// Padded shared-memory index: one spare slot every E elements keeps the
-// first pass's stride-E writes free of bank conflicts.
-template <int E>
-__device__ __forceinline__ int spad(int a) {
-  return a + (a >> ilog2c<E>());
+// Shared-memory index of element a in the exchange after a pass of span ns.
+// Elements are stored unpadded; within each 128-byte row (Q = 128 /
+// sizeof(C) elements) the slot is XOR-swizzled so that both access patterns
+// of the exchange are free of bank conflicts:
+//   writes  a = (t/ns)*ns*E + t%ns + r*ns   (the radix-E butterfly outputs)
+//   reads   a = t + e*P                      (consecutive threads)
+// For ns >= Q the writes already come in runs of Q consecutive elements and
+// no swizzle is needed.  Otherwise the bits of a that select the butterfly
+// group (bits log2(ns*E)...) are folded into the slot bits above log2(ns).
+template <int E, int Q>
+__device__ __forceinline__ int sswz(int a, int ns) {
+  if (ns >= Q) return a;
+  const int mask = ((Q / ns) - 1) * ns;  // slot bits above log2(ns)
+  return a ^ ((a >> ilog2c<E>()) & mask);
 }
 template <int N, int E>
 __host__ __device__ constexpr int line_smem_elems() {
-  return N + N / E;
+  return N;
 }
 
 // Twiddle exp(-+2 pi i a*scale / N) from the length-N table.
@@ -213,6 +238,18 @@ __device__ __forceinline__ C twid(const C* __restrict__ tw, int a, int scale) {
   C w = __ldg(&tw[a * scale]);
   if (INV) w.y = -w.y;
   return w;
+}
+
+// Barrier among the threads of one line.  A line of P <= 32 threads lies
+// inside one warp (lines are consecutive thread ranges of power-of-two size),
+// so a warp barrier suffices; larger lines use the block barrier, which every
+// thread of the block reaches because all lines run the same passes.
+template <int P>
+__device__ __forceinline__ void line_sync() {
+  if (P <= 32)
+    __syncwarp();
+  else
+    __syncthreads();
 }
 
 template <int N, int E>
@@ -225,7 +262,7 @@ struct LinePlan {
 };
 
 // Runs the line FFT in place on v.  All threads of the block must call it
-// (it contains __syncthreads); sm is this line's padded buffer of
+// (it contains barriers); sm is this line's buffer of
 // line_smem_elems<N,E>() elements; tw is the length-N twiddle table.
 template <typename T, int N, int E, bool INV>
 __device__ __forceinline__ void line_fft(cpx<T> (&v)[E], cpx<T>* sm, int t, const cpx<T>* __restrict__ tw) {
@@ -246,13 +283,14 @@ __device__ __forceinline__ void line_fft(cpx<T> (&v)[E], cpx<T>* sm, int t, cons
     dft<E, INV>(v);
     const bool last = (s == SF - 1) && (RL == 1);
     if (!last) {
-      __syncthreads();
+      constexpr int Q = 128 / (int)sizeof(C);
+      line_sync<P>();
       const int base = (t / ns) * ns * E + (t & (ns - 1));
 #pragma unroll
-      for (int r = 0; r < E; r++) sm[spad<E>(base + r * ns)] = v[r];
-      __syncthreads();
+      for (int r = 0; r < E; r++) sm[sswz<E, Q>(base + r * ns, ns)] = v[r];
+      line_sync<P>();
 #pragma unroll
-      for (int e = 0; e < E; e++) v[e] = sm[spad<E>(t + e * P)];
+      for (int e = 0; e < E; e++) v[e] = sm[sswz<E, Q>(t + e * P, ns)];
     }
     ns *= E;
   }

@@ -20,6 +20,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <cstdlib>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -28,18 +29,26 @@
 #include "hos_registry.h"
 
 namespace hos {
-XInvFn lookup_xinv_64(int mode, int n);
-XFwdFn lookup_xfwd_64(int mode, int n);
-YInvFn lookup_yinv_64(int mode, int h);
-YFwdFn lookup_yfwd_64(int mode, int h);
-XInvFn lookup_xinv_32(int mode, int n);
-XFwdFn lookup_xfwd_32(int mode, int n);
-YInvFn lookup_yinv_32(int mode, int h);
-YFwdFn lookup_yfwd_32(int mode, int h);
-XInvFn lookup_xinv(int prec, int mode, int n) { return prec ? lookup_xinv_32(mode, n) : lookup_xinv_64(mode, n); }
-XFwdFn lookup_xfwd(int prec, int mode, int n) { return prec ? lookup_xfwd_32(mode, n) : lookup_xfwd_64(mode, n); }
-YInvFn lookup_yinv(int prec, int mode, int h) { return prec ? lookup_yinv_32(mode, h) : lookup_yinv_64(mode, h); }
-YFwdFn lookup_yfwd(int prec, int mode, int h) { return prec ? lookup_yfwd_32(mode, h) : lookup_yfwd_64(mode, h); }
+XInvFn lookup_xinv_64(int mode, int n, int e);
+XFwdFn lookup_xfwd_64(int mode, int n, int e);
+YInvFn lookup_yinv_64(int mode, int h, int e);
+YFwdFn lookup_yfwd_64(int mode, int h, int e);
+XInvFn lookup_xinv_32(int mode, int n, int e);
+XFwdFn lookup_xfwd_32(int mode, int n, int e);
+YInvFn lookup_yinv_32(int mode, int h, int e);
+YFwdFn lookup_yfwd_32(int mode, int h, int e);
+XInvFn lookup_xinv(int prec, int mode, int n, int e) {
+  return prec ? lookup_xinv_32(mode, n, e) : lookup_xinv_64(mode, n, e);
+}
+XFwdFn lookup_xfwd(int prec, int mode, int n, int e) {
+  return prec ? lookup_xfwd_32(mode, n, e) : lookup_xfwd_64(mode, n, e);
+}
+YInvFn lookup_yinv(int prec, int mode, int h, int e) {
+  return prec ? lookup_yinv_32(mode, h, e) : lookup_yinv_64(mode, h, e);
+}
+YFwdFn lookup_yfwd(int prec, int mode, int h, int e) {
+  return prec ? lookup_yfwd_32(mode, h, e) : lookup_yfwd_64(mode, h, e);
+}
 
 // ---------------------------------------------------------------- small kernels
 __global__ void k_set_int(int* p, int v) {
@@ -125,18 +134,29 @@ static int fail(int code, const char* fmt, ...) {
 // ---------------------------------------------------------------- plan
 namespace {
 
+// Launch geometry of one pass kind: elements per thread E, lines per block,
+// threads, dynamic shared memory and (y-passes) the line pitch.
+struct KindCfg {
+  int e = 8;
+  int lines = 1, threads = 0, lp = 0;
+  size_t smem = 0;
+};
+
 struct PassCfg {
   XInvFn xinv[2] = {};
   XFwdFn xfwd[3] = {};
   YInvFn yinv[2] = {};
   YFwdFn yfwd[3] = {};
-  int xlines = 1, xthreads = 0;
-  size_t xsmem = 0;
-  int ylines = 1, ythreads = 0, ylp = 0;
-  size_t ysmem = 0;
+  KindCfg xi, xf, yi, yf;
   const void* twx = nullptr;  // length nx
   const void* twh = nullptr;  // length ny/2
   const void* twy = nullptr;  // length ny
+};
+
+// Elements per thread of each pass kind (x-inverse, x-forward, y-inverse,
+// y-forward); defaults, overridable per handle by the autotuner.
+struct ElemChoice {
+  int xi = 8, xf = 8, yi = 8, yf = 8;
 };
 
 int ilog2i(int n) {
@@ -289,54 +309,89 @@ struct hos_ctx {
 
 namespace {
 
-int make_cfg(hos_ctx* c, int prec, PassCfg* o) {
-  for (int m = 0; m < 2; m++) o->xinv[m] = lookup_xinv(prec, m, c->nx);
-  for (int m = 0; m < 3; m++) o->xfwd[m] = lookup_xfwd(prec, m, c->nx);
-  for (int m = 0; m < 2; m++) o->yinv[m] = lookup_yinv(prec, m, c->h);
-  for (int m = 0; m < 3; m++) o->yfwd[m] = lookup_yfwd(prec, m, c->h);
+int x_geometry(int n, int e, size_t cs, KindCfg* k) {
+  const int P = n / e;
+  int lines = 128 / P;
+  if (lines < 1) lines = 1;
+  k->e = e;
+  k->lines = lines;
+  k->threads = lines * P;
+  k->smem = (size_t)lines * (size_t)n * cs;
+  if (k->threads % 32 != 0 || k->threads > MAX_THREADS) return -1;
+  return 0;
+}
+
+int y_geometry(int h, int nx, int e, size_t cs, KindCfg* k) {
+  const int P = h / e;
+  int lines = MAX_THREADS / P;
+  if (lines > nx) lines = nx;
+  if (lines < 1) lines = 1;
+  k->e = e;
+  k->lines = lines;
+  k->threads = lines * P;
+  const int phase = (int)(128 / cs);
+  const int target = lines >= phase ? 1 : phase / lines;
+  int lp = h + 1;
+  while (lp % phase != target % phase) lp++;
+  k->lp = lp;
+  k->smem = (size_t)lines * lp * cs;
+  return k->threads > MAX_THREADS ? -1 : 0;
+}
+
+// Largest supported E not above `want` for a line of length n.
+int pick_elems(int prec, int n, int want) {
+  for (int e = want; e >= 8; e >>= 1)
+    if (elems_valid(prec, n, e)) return e;
+  return elems_valid(prec, n, 16) ? 16 : 32;
+}
+
+// Defaults: E = 8 for every pass kind measured fastest on B200 at 1024^2 in
+// both precisions; overridable through HOS_ELEMS="xi,xf,yi,yf".
+ElemChoice default_elems(int prec) {
+  (void)prec;
+  ElemChoice ec;
+  if (const char* s = getenv("HOS_ELEMS")) {
+    int a[4];
+    if (sscanf(s, "%d,%d,%d,%d", &a[0], &a[1], &a[2], &a[3]) == 4) {
+      ec.xi = a[0];
+      ec.xf = a[1];
+      ec.yi = a[2];
+      ec.yf = a[3];
+    }
+  }
+  return ec;
+}
+
+int make_cfg(hos_ctx* c, int prec, const ElemChoice& ec, PassCfg* o) {
+  const size_t cs = prec ? sizeof(float2) : sizeof(double2);
+  const int exi = pick_elems(prec, c->nx, ec.xi), exf = pick_elems(prec, c->nx, ec.xf);
+  const int eyi = pick_elems(prec, c->h, ec.yi), eyf = pick_elems(prec, c->h, ec.yf);
+  for (int m = 0; m < 2; m++) o->xinv[m] = lookup_xinv(prec, m, c->nx, exi);
+  for (int m = 0; m < 3; m++) o->xfwd[m] = lookup_xfwd(prec, m, c->nx, exf);
+  for (int m = 0; m < 2; m++) o->yinv[m] = lookup_yinv(prec, m, c->h, eyi);
+  for (int m = 0; m < 3; m++) o->yfwd[m] = lookup_yfwd(prec, m, c->h, eyf);
   for (int m = 0; m < 3; m++)
     if (!o->xfwd[m] || !o->yfwd[m] || (m < 2 && (!o->xinv[m] || !o->yinv[m])))
-      return fail(HOS_ERR_ARG, "no kernels for %dx%d", c->nx, c->ny);
-  const size_t cs = prec ? sizeof(float2) : sizeof(double2);
-  {
-    const int E = elems_for(c->nx), P = c->nx / E;
-    int lines = 128 / P;
-    if (lines < 1) lines = 1;
-    o->xlines = lines;
-    o->xthreads = lines * P;
-    o->xsmem = (size_t)lines * (size_t)(c->nx + c->nx / E) * cs;
-  }
-  {
-    const int E = elems_for(c->h), P = c->h / E;
-    int lines = MAX_THREADS / P;
-    if (lines > c->nx) lines = c->nx;
-    if (lines < 1) lines = 1;
-    o->ylines = lines;
-    o->ythreads = lines * P;
-    const int phase = (int)(128 / cs);
-    const int target = lines >= phase ? 1 : phase / lines;
-    int lp = c->h + c->h / E + 1;
-    while (lp % phase != target % phase) lp++;
-    o->ylp = lp;
-    o->ysmem = (size_t)lines * lp * cs;
-  }
-  if (o->xthreads % 32 != 0) return fail(HOS_ERR_ARG, "x-pass block of %d threads", o->xthreads);
+      return fail(HOS_ERR_ARG, "no kernels for %dx%d (E %d/%d/%d/%d)", c->nx, c->ny, exi, exf, eyi, eyf);
+  if (x_geometry(c->nx, exi, cs, &o->xi) || x_geometry(c->nx, exf, cs, &o->xf) ||
+      y_geometry(c->h, c->nx, eyi, cs, &o->yi) || y_geometry(c->h, c->nx, eyf, cs, &o->yf))
+    return fail(HOS_ERR_ARG, "no launch geometry for %dx%d", c->nx, c->ny);
   for (int m = 0; m < 2; m++)
-    HOS_CK(cudaFuncSetAttribute((const void*)o->xinv[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->xsmem));
+    HOS_CK(cudaFuncSetAttribute((const void*)o->xinv[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->xi.smem));
   for (int m = 0; m < 3; m++)
-    HOS_CK(cudaFuncSetAttribute((const void*)o->xfwd[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->xsmem));
+    HOS_CK(cudaFuncSetAttribute((const void*)o->xfwd[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->xf.smem));
   for (int m = 0; m < 2; m++)
-    HOS_CK(cudaFuncSetAttribute((const void*)o->yinv[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->ysmem));
+    HOS_CK(cudaFuncSetAttribute((const void*)o->yinv[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->yi.smem));
   for (int m = 0; m < 3; m++)
-    HOS_CK(cudaFuncSetAttribute((const void*)o->yfwd[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->ysmem));
+    HOS_CK(cudaFuncSetAttribute((const void*)o->yfwd[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->yf.smem));
   o->twx = c->tw[prec][0];
   o->twh = c->tw[prec][1];
   o->twy = c->tw[prec][2];
   return HOS_OK;
 }
 
-inline int xgrid(const hos_ctx* c, const PassCfg& g) { return (c->h + 1 + g.xlines - 1) / g.xlines; }
-inline int ygrid(const hos_ctx* c, const PassCfg& g) { return c->nx / g.ylines; }
+inline int xgrid(const hos_ctx* c, const KindCfg& k) { return (c->h + 1 + k.lines - 1) / k.lines; }
+inline int ygrid(const hos_ctx* c, const KindCfg& k) { return c->nx / k.lines; }
 
 size_t compute_bytes(const hos_params* p, int nst) {
   const size_t nx = p->nx, ny = p->ny, h = ny / 2;
@@ -392,7 +447,6 @@ int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, dou
   char* zb = reinterpret_cast<char*>(c->zbuf);
   const double act = lg ? (double)lg->act_rows : 0.0;
   const double nxd = (double)c->nx, psz = (double)c->psz, fszd = (double)fsz, my = (double)c->geo.my;
-  const int gx = xgrid(c, g), gy = ygrid(c, g);
 
   XInvArgs xa{};
   xa.geo = c->geo;
@@ -415,12 +469,12 @@ int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, dou
   xa.set_ramp = (s == 0);
   xa.tramp = c->p.tramp;
   xa.rampflg = c->p.rampflg;
-  g.xinv[XI_STAGE]<<<dim3(gx, 4 + M), g.xthreads, g.xsmem, c->st>>>(xa, g.twx);
+  g.xinv[XI_STAGE]<<<dim3(xgrid(c, g.xi), 4 + M), g.xi.threads, g.xi.smem, c->st>>>(xa, g.twx);
   log_pass(c, lg, P_XINV_STAGE, act * nxd * (16.0 * 2 * (1 + nk) + (double)cs * (4 + M)));
 
   YInvArgs ya{};
   ya.geo = c->geo;
-  ya.lp = g.ylp;
+  ya.lp = g.yi.lp;
   ya.z = c->zbuf;
   ya.rows_in = c->h + 1;
   ya.rows_dev = rows_dev;
@@ -432,23 +486,20 @@ int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, dou
   ya.jobs[nj++] = YJob{2, 1, c->PHIY()};
   ya.jobs[nj++] = YJob{3, 0, c->PHIX()};
   for (int j = 1; j <= M; j++) ya.jobs[nj++] = YJob{4 + j - 1, 0, c->D(1, j)};
-  g.yinv[YI_JOBS]<<<dim3(gy, nj), g.ythreads, g.ysmem, c->st>>>(ya, g.twh, g.twy);
+  g.yinv[YI_JOBS]<<<dim3(ygrid(c, g.yi), nj), g.yi.threads, g.yi.smem, c->st>>>(ya, g.twh, g.twy);
   log_pass(c, lg, P_YINV_STAGE, act * nxd * (double)cs * (4 + M) + psz * (double)rs * (5 + M));
 
   for (int n = 1; n <= L; n++) {
     YFwdArgs fa{};
     fa.geo = c->geo;
-    fa.lp = g.ylp;
+    fa.lp = g.yf.lp;
     fa.phys = c->phys;
     fa.eta = c->ETA();
     fa.nterms = n;
-    for (int m = 0; m < n; m++) {
-      fa.t_in[m] = c->D(m + 1, n - m);
-      fa.t_pow[m] = n - m;
-    }
+    for (int p = 1; p <= n; p++) fa.t_in[p - 1] = c->D(n - p + 1, p);  // power p: m = n - p
     fa.vout = zb;
     fa.rows_out = c->h + 1;
-    g.yfwd[YF_LEVEL]<<<dim3(gy, 1), g.ythreads, g.ysmem, c->st>>>(fa, g.twh, g.twy);
+    g.yfwd[YF_LEVEL]<<<dim3(ygrid(c, g.yf), 1), g.yf.threads, g.yf.smem, c->st>>>(fa, g.twh, g.twy);
     log_pass(c, lg, P_YFWD_LEVEL, psz * (double)rs * (n + 1) + fszd * (double)cs);
 
     XFwdArgs xf{};
@@ -456,13 +507,12 @@ int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, dou
     xf.rows = c->h + 1;
     xf.vin0 = zb;
     xf.zout = zb + fsz * cs;
-    xf.ndz = M - n;
-    g.xfwd[XF_LEVEL]<<<dim3(gx, 1), g.xthreads, g.xsmem, c->st>>>(xf, g.twx);
+    g.xfwd[XF_LEVEL]<<<dim3(xgrid(c, g.xf), M - n), g.xf.threads, g.xf.smem, c->st>>>(xf, g.twx);
     log_pass(c, lg, P_XFWD_LEVEL, fszd * (double)cs * (1 + M - n));
 
     YInvArgs yl{};
     yl.geo = c->geo;
-    yl.lp = g.ylp;
+    yl.lp = g.yi.lp;
     yl.z = c->zbuf;
     yl.rows_in = c->h + 1;
     yl.phys = c->phys;
@@ -471,17 +521,14 @@ int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, dou
     yl.w_out = c->W(n);
     yl.eta = c->ETA();
     yl.w_terms = n;
-    for (int m = 0; m < n; m++) {
-      yl.w_in[m] = c->D(m + 1, n - m + 1);
-      yl.w_pow[m] = n - m;
-    }
-    g.yinv[YI_LEVEL]<<<dim3(gy, nl), g.ythreads, g.ysmem, c->st>>>(yl, g.twh, g.twy);
+    for (int p = 1; p <= n; p++) yl.w_in[p - 1] = c->D(n - p + 1, p + 1);  // power p: m = n - p
+    g.yinv[YI_LEVEL]<<<dim3(ygrid(c, g.yi), nl), g.yi.threads, g.yi.smem, c->st>>>(yl, g.twh, g.twy);
     log_pass(c, lg, P_YINV_LEVEL, fszd * (double)cs * (M - n) + psz * (double)rs * (M - n + 1 + n + 1));
   }
 
   YFwdArgs ff{};
   ff.geo = c->geo;
-  ff.lp = g.ylp;
+  ff.lp = g.yf.lp;
   ff.phys = c->phys;
   ff.ex = c->ETAX();
   ff.ey = c->ETAY();
@@ -491,7 +538,7 @@ int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, dou
   for (int n = 0; n <= L; n++) ff.w_idx[n] = c->W(n);
   ff.vout = zb;
   ff.rows_out = c->geo.my;
-  g.yfwd[YF_RHS]<<<dim3(gy, 2), g.ythreads, g.ysmem, c->st>>>(ff, g.twh, g.twy);
+  g.yfwd[YF_RHS]<<<dim3(ygrid(c, g.yf), 2), g.yf.threads, g.yf.smem, c->st>>>(ff, g.twh, g.twy);
   log_pass(c, lg, P_YFWD_RHS, psz * (double)rs * (5 + L) + 2.0 * my * nxd * (double)cs);
 
   XFwdArgs xe{};
@@ -513,7 +560,7 @@ int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, dou
     xe.cfin[p] = dt * c->c[p];
   }
   xe.nstage = c->nst;
-  g.xfwd[XF_RHS]<<<dim3(gx, 2), g.xthreads, g.xsmem, c->st>>>(xe, g.twx);
+  g.xfwd[XF_RHS]<<<dim3(xgrid(c, g.xf), 2), g.xf.threads, g.xf.smem, c->st>>>(xe, g.twx);
   {
     // V rows < my in, stage input (u + earlier k) rows < act, k_s rows < my out;
     // on the last stage also the other k's and the updated u (rows < my)
@@ -529,7 +576,7 @@ int enqueue_step(hos_ctx* c, double dt) {
     int rc = enqueue_stage(c, s, dt, false, c->u, c->k + (size_t)s * 2 * c->fsz, c->tdev, c->actdev);
     if (rc) return rc;
   }
-  k_step_end<<<1, 256, 0, c->st>>>(c->ham_part, xgrid(c, c->cfg), c->tdev, dt, c->stepdev, c->ham_hist, c->t_hist,
+  k_step_end<<<1, 256, 0, c->st>>>(c->ham_part, xgrid(c, c->cfg.xf), c->tdev, dt, c->stepdev, c->ham_hist, c->t_hist,
                                   HIST_CAP);
   return HOS_OK;
 }
@@ -566,18 +613,18 @@ int enqueue_r2c(hos_ctx* c, const double* phys_in, double2* spec_out, int dealia
   const PassCfg& g = c->cfg64;
   YFwdArgs fa{};
   fa.geo = c->geo;
-  fa.lp = g.ylp;
+  fa.lp = g.yf.lp;
   fa.in_ptr = phys_in;
   fa.vout = c->zplain;
   fa.rows_out = c->h + 1;
-  g.yfwd[YF_PLAIN]<<<dim3(ygrid(c, g), 1), g.ythreads, g.ysmem, c->st>>>(fa, g.twh, g.twy);
+  g.yfwd[YF_PLAIN]<<<dim3(ygrid(c, g.yf), 1), g.yf.threads, g.yf.smem, c->st>>>(fa, g.twh, g.twy);
   XFwdArgs xf{};
   xf.geo = c->geo;
   xf.rows = c->h + 1;
   xf.vin0 = c->zplain;
   xf.out_spec = spec_out;
   xf.dealias = dealias;
-  g.xfwd[XF_PLAIN]<<<dim3(xgrid(c, g), 1), g.xthreads, g.xsmem, c->st>>>(xf, g.twx);
+  g.xfwd[XF_PLAIN]<<<dim3(xgrid(c, g.xf), 1), g.xf.threads, g.xf.smem, c->st>>>(xf, g.twx);
   return HOS_OK;
 }
 
@@ -588,15 +635,15 @@ int enqueue_c2r(hos_ctx* c, const double2* spec_in, double* phys_out) {
   xa.rows = c->h + 1;
   xa.u = spec_in;
   xa.z = c->zplain;
-  g.xinv[XI_PLAIN]<<<dim3(xgrid(c, g), 1), g.xthreads, g.xsmem, c->st>>>(xa, g.twx);
+  g.xinv[XI_PLAIN]<<<dim3(xgrid(c, g.xi), 1), g.xi.threads, g.xi.smem, c->st>>>(xa, g.twx);
   YInvArgs ya{};
   ya.geo = c->geo;
-  ya.lp = g.ylp;
+  ya.lp = g.yi.lp;
   ya.z = c->zplain;
   ya.rows_in = c->h + 1;
   ya.phys = phys_out;
   ya.jobs[0] = YJob{0, 0, 0};
-  g.yinv[YI_JOBS]<<<dim3(ygrid(c, g), 1), g.ythreads, g.ysmem, c->st>>>(ya, g.twh, g.twy);
+  g.yinv[YI_JOBS]<<<dim3(ygrid(c, g.yi), 1), g.yi.threads, g.yi.smem, c->st>>>(ya, g.twh, g.twy);
   return HOS_OK;
 }
 
@@ -749,13 +796,17 @@ int hos_create(const hos_params* p, hos_handle* out) {
   HOS_AL(c->ham_hist, HIST_CAP * sizeof(double));
   HOS_AL(c->t_hist, HIST_CAP * sizeof(double));
 #undef HOS_AL
-  rc = make_cfg(c, c->prec, &c->cfg);
-  if (!rc) rc = make_cfg(c, 0, &c->cfg64);
+  {
+    ElemChoice ec = default_elems(c->prec);
+    ElemChoice ec64 = default_elems(0);
+    rc = make_cfg(c, c->prec, ec, &c->cfg);
+    if (!rc) rc = make_cfg(c, 0, ec64, &c->cfg64);
+  }
   if (rc) {
     release(c);
     return rc;
   }
-  c->nparts = xgrid(c, c->cfg);
+  c->nparts = xgrid(c, c->cfg.xf);
   rc = dalloc(&c->ham_part, (size_t)c->nparts * sizeof(double));
   if (rc) {
     release(c);

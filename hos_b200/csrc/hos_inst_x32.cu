@@ -3,43 +3,74 @@
 
 namespace hos {
 
-#define HOS_SIZES(F) F(16) F(32) F(64) F(128) F(256) F(512) F(1024) F(2048) F(4096)
 
-#define HOS_CASE(N) \
-  case N:           \
-    return &k_xinv<float, N, elems_for(N), M>;
-template <int M>
+template <int N, int E, int M>
+constexpr XInvFn xinv_fn() {
+  if constexpr (elems_valid(1, N, E)) return &k_xinv<float, N, E, M>;
+  else return nullptr;
+}
+template <int N, int E, int M>
+constexpr XFwdFn xfwd_fn() {
+  if constexpr (elems_valid(1, N, E)) return &k_xfwd<float, N, E, M>;
+  else return nullptr;
+}
+
+#define HOS_SIZES(F, E, M) F(16, E, M) F(32, E, M) F(64, E, M) F(128, E, M) F(256, E, M) F(512, E, M) \
+  F(1024, E, M) F(2048, E, M) F(4096, E, M)
+
+#define HOS_CASE_I(N, E, M) \
+  case N:                   \
+    return xinv_fn<N, E, M>();
+#define HOS_CASE_F(N, E, M) \
+  case N:                   \
+    return xfwd_fn<N, E, M>();
+
+template <int E, int M>
 static XInvFn xinv_n(int n) {
   switch (n) {
-    HOS_SIZES(HOS_CASE)
+    HOS_SIZES(HOS_CASE_I, E, M)
     default: return nullptr;
   }
 }
-#undef HOS_CASE
-#define HOS_CASE(N) \
-  case N:           \
-    return &k_xfwd<float, N, elems_for(N), M>;
-template <int M>
+template <int E, int M>
 static XFwdFn xfwd_n(int n) {
   switch (n) {
-    HOS_SIZES(HOS_CASE)
+    HOS_SIZES(HOS_CASE_F, E, M)
     default: return nullptr;
   }
 }
-#undef HOS_CASE
 
-XInvFn lookup_xinv_32(int mode, int n) {
-  switch (mode) {
-    case XI_STAGE: return xinv_n<XI_STAGE>(n);
-    case XI_PLAIN: return xinv_n<XI_PLAIN>(n);
+template <int M>
+static XInvFn xinv_e(int n, int e) {
+  switch (e) {
+    case 8: return xinv_n<8, M>(n);
+    case 16: return xinv_n<16, M>(n);
+    case 32: return xinv_n<32, M>(n);
     default: return nullptr;
   }
 }
-XFwdFn lookup_xfwd_32(int mode, int n) {
+template <int M>
+static XFwdFn xfwd_e(int n, int e) {
+  switch (e) {
+    case 8: return xfwd_n<8, M>(n);
+    case 16: return xfwd_n<16, M>(n);
+    case 32: return xfwd_n<32, M>(n);
+    default: return nullptr;
+  }
+}
+
+XInvFn lookup_xinv_32(int mode, int n, int e) {
   switch (mode) {
-    case XF_PLAIN: return xfwd_n<XF_PLAIN>(n);
-    case XF_LEVEL: return xfwd_n<XF_LEVEL>(n);
-    case XF_RHS: return xfwd_n<XF_RHS>(n);
+    case XI_STAGE: return xinv_e<XI_STAGE>(n, e);
+    case XI_PLAIN: return xinv_e<XI_PLAIN>(n, e);
+    default: return nullptr;
+  }
+}
+XFwdFn lookup_xfwd_32(int mode, int n, int e) {
+  switch (mode) {
+    case XF_PLAIN: return xfwd_e<XF_PLAIN>(n, e);
+    case XF_LEVEL: return xfwd_e<XF_LEVEL>(n, e);
+    case XF_RHS: return xfwd_e<XF_RHS>(n, e);
     default: return nullptr;
   }
 }

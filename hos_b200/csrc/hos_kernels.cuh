@@ -166,8 +166,7 @@ struct XFwdArgs {
   const void* vin1;
   double2* out_spec;    // PLAIN output
   int dealias;          // PLAIN: zero the modes Dealias zeroes (operators_par.c:283-325)
-  void* zout;           // LEVEL: output Z arrays (T2), stride (h+1)*nx
-  int ndz;              // LEVEL: z-derivative orders 1..ndz
+  void* zout;           // LEVEL: output Z arrays (T2), stride (h+1)*nx; order blockIdx.y+1
   // RHS
   double2* u;                     // packed state at step start (updated in place on the final stage)
   const double2* ustg;            // stage input of both fields, written by the x-inverse pass
@@ -218,21 +217,21 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_xfwd(const __grid_constant__
       }
       return;
     }
-    // LEVEL: v holds phi^(n+1) hat; emit its z-derivatives of orders 1..ndz
+    // LEVEL: v holds phi^(n+1) hat; this block emits its z-derivative of
+    // order p = blockIdx.y + 1 (the forward transform is repeated per order
+    // so that the orders run in parallel blocks)
     const double ky = ky_of(geo, row);
-    C* z = reinterpret_cast<C*>(a.zout);
-    for (int p = 1; p <= a.ndz; p++) {
-      C w[E];
+    const int p = blockIdx.y + 1;
+    C* z = reinterpret_cast<C*>(a.zout) + (size_t)(p - 1) * fsz;
 #pragma unroll
-      for (int e = 0; e < E; e++) {
-        const double kx = kx_of(geo, t + e * P);
-        w[e] = cscale(v[e], (T)dz_mult(geo, sqrt(kx * kx + ky * ky), p));
-      }
-      line_fft<T, NX, E, true>(w, sm, t, tw);
-      if (live) {
+    for (int e = 0; e < E; e++) {
+      const double kx = kx_of(geo, t + e * P);
+      v[e] = cscale(v[e], (T)dz_mult(geo, sqrt(kx * kx + ky * ky), p));
+    }
+    line_fft<T, NX, E, true>(v, sm, t, tw);
+    if (live) {
 #pragma unroll
-        for (int e = 0; e < E; e++) z[(size_t)(p - 1) * fsz + roff + t + e * P] = w[e];
-      }
+      for (int e = 0; e < E; e++) z[roff + t + e * P] = v[e];
     }
     return;
   }
@@ -314,10 +313,9 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_xfwd(const __grid_constant__
 
 // ---------------------------------------------------------------- y passes
 // Shared memory of a y-pass block: G line regions of `lp` complex elements.
-// A line region first holds the line's spectral column (index ky, padded by
-// spad) and then serves as the line FFT's exchange buffer.  lp >= h + h/E + 1
-// and lp is chosen so that the G-wide column strips move without bank
-// conflicts.
+// A line region first holds the line's spectral column (index ky) and then
+// serves as the line FFT's exchange buffer.  lp >= h + 1 and lp is chosen so
+// that the G-wide column strips move without bank conflicts.
 
 struct YJob {
   int zin;  // input Z array index
@@ -334,13 +332,12 @@ struct YInvArgs {
   void* phys;        // physical arrays (T), stride nx*ny
   YJob jobs[MAX_JOBS];  // job of a block = jobs[blockIdx.y]
   // LEVEL: the block of job 0 (order-1 derivative of phi^(n+1)) also forms
-  // W_n = job0 + sum_q phys[w_in[q]] * eta^w_pow[q] / w_pow[q]!
+  // W_n = job0 + sum_q phys[w_in[q]] * eta^(q+1) / (q+1)!
   // (hosm_2d_par.c:322-357 restated in physical space)
   int w_out;
   int eta;
   int w_terms;
   int w_in[MAX_TERMS];
-  int w_pow[MAX_TERMS];
 };
 
 template <typename T, int H, int E, int MODE>
@@ -372,7 +369,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yinv(const __grid_constant__
     const int ntot = G * (H + 1);
     for (int q = threadIdx.x; q < ntot; q += blockDim.x) {
       const int ky = q / G, g = q - ky * G;
-      sm[(size_t)g * a.lp + spad<E>(ky)] = (q < nin) ? zs[(size_t)ky * nx + ix0 + g] : mkc((T)0, (T)0);
+      sm[(size_t)g * a.lp + (ky)] = (q < nin) ? zs[(size_t)ky * nx + ix0 + g] : mkc((T)0, (T)0);
     }
   }
   __syncthreads();
@@ -382,8 +379,8 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yinv(const __grid_constant__
 #pragma unroll
   for (int e = 0; e < E; e++) {
     const int k = t + e * P;
-    C A = tl[spad<E>(k)];
-    C B = tl[spad<E>(H - k)];
+    C A = tl[(k)];
+    C B = tl[(H - k)];
     if (J.iky) {
       const T ka = (T)ky_of(geo, k), kb = (T)ky_of(geo, H - k);
       A = cscale(cmul_i(A), ka);
@@ -405,28 +402,29 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yinv(const __grid_constant__
 #pragma unroll
   for (int e = 0; e < E; e++) po[t + e * P] = v[e];
   if (MODE == YI_LEVEL && blockIdx.y == 0) {
+    // terms ordered by power 1, 2, ..., w_terms (host side); p = eta^k/k!
     const C* pe = reinterpret_cast<const C*>(pall + (size_t)a.eta * psz + (size_t)ix * ny);
-    C* pw = reinterpret_cast<C*>(pall + (size_t)a.w_out * psz + (size_t)ix * ny);
+    C* pwo = reinterpret_cast<C*>(pall + (size_t)a.w_out * psz + (size_t)ix * ny);
+    C et[E], p[E];
 #pragma unroll
     for (int e = 0; e < E; e++) {
-      const int m = t + e * P;
-      const C et = pe[m];
-      C acc = mkc((T)0, (T)0);
-      for (int q = 0; q < a.w_terms; q++) {
-        const C d = reinterpret_cast<const C*>(pall + (size_t)a.w_in[q] * psz + (size_t)ix * ny)[m];
-        T px = (T)1, py = (T)1, fct = (T)1;
-        for (int r = 1; r <= a.w_pow[q]; r++) {
-          px *= et.x;
-          py *= et.y;
-          fct *= (T)r;
-        }
-        acc.x += d.x * px / fct;
-        acc.y += d.y * py / fct;
-      }
-      acc.x += v[e].x;
-      acc.y += v[e].y;
-      pw[m] = acc;
+      et[e] = pe[t + e * P];
+      p[e] = mkc((T)1, (T)1);
     }
+    for (int q = 0; q < a.w_terms; q++) {
+      const C* pd = reinterpret_cast<const C*>(pall + (size_t)a.w_in[q] * psz + (size_t)ix * ny);
+      const T inv = (T)1 / (T)(q + 1);
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        const C d = pd[t + e * P];
+        p[e].x = p[e].x * et[e].x * inv;
+        p[e].y = p[e].y * et[e].y * inv;
+        v[e].x += d.x * p[e].x;
+        v[e].y += d.y * p[e].y;
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < E; e++) pwo[t + e * P] = v[e];
   }
 }
 
@@ -435,11 +433,10 @@ struct YFwdArgs {
   int lp;
   const void* phys;   // physical arrays (T), stride nx*ny
   const void* in_ptr; // PLAIN: physical input (T) [nx][ny]
-  // LEVEL: P = -sum_q phys[t_in[q]] * eta^t_pow[q] / t_pow[q]!  (hosm_2d_par.c:302-317)
+  // LEVEL: P = -sum_q phys[t_in[q]] * eta^(q+1) / (q+1)!  (hosm_2d_par.c:302-317)
   int eta;
   int nterms;
   int t_in[MAX_TERMS];
-  int t_pow[MAX_TERMS];
   // RHS (blockIdx.y = 0: P_eta, 1: P_phi)
   int ex, ey, px, py;
   int L;
@@ -450,12 +447,8 @@ struct YFwdArgs {
 
 // RHS assembly at one physical point: P_eta (which = 0) or P_phi (which = 1).
 template <typename T>
-__device__ __forceinline__ T rhs_point(const YFwdArgs& a, const T* const* Wp, size_t off, T ex, T ey, T px, T py,
-                                       int which) {
-  T W[MAX_TERMS];
+__device__ __forceinline__ T rhs_point(const YFwdArgs& a, const T* W, T ex, T ey, T px, T py, int which) {
   const int L = a.L;
-#pragma unroll
-  for (int n = 0; n < MAX_TERMS; n++) W[n] = (n <= L) ? Wp[n][off] : (T)0;
   const T grad2 = ex * ex + ey * ey;
   if (which == 0) {
     T s1 = (T)0, wm2 = (T)0;
@@ -510,40 +503,47 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yfwd(const __grid_constant__
 #pragma unroll
     for (int e = 0; e < E; e++) v[e] = src[t + e * P];
   } else if (MODE == YF_LEVEL) {
+    // terms are ordered by power 1, 2, ..., nterms (host side); pw = eta^p/p!
     const C* pe = reinterpret_cast<const C*>(pall + (size_t)a.eta * psz + rowoff);
+    C et[E], pw[E];
 #pragma unroll
     for (int e = 0; e < E; e++) {
-      const int m = t + e * P;
-      const C et = pe[m];
-      C acc = mkc((T)0, (T)0);
-      for (int q = 0; q < a.nterms; q++) {
-        const C d = reinterpret_cast<const C*>(pall + (size_t)a.t_in[q] * psz + rowoff)[m];
-        T px = (T)1, py = (T)1, fct = (T)1;
-        for (int r = 1; r <= a.t_pow[q]; r++) {
-          px *= et.x;
-          py *= et.y;
-          fct *= (T)r;
-        }
-        acc.x -= d.x * px / fct;
-        acc.y -= d.y * py / fct;
+      et[e] = pe[t + e * P];
+      pw[e] = mkc((T)1, (T)1);
+      v[e] = mkc((T)0, (T)0);
+    }
+    for (int q = 0; q < a.nterms; q++) {
+      const C* pd = reinterpret_cast<const C*>(pall + (size_t)a.t_in[q] * psz + rowoff);
+      const T inv = (T)1 / (T)(q + 1);
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        const C d = pd[t + e * P];
+        pw[e].x = pw[e].x * et[e].x * inv;
+        pw[e].y = pw[e].y * et[e].y * inv;
+        v[e].x -= d.x * pw[e].x;
+        v[e].y -= d.y * pw[e].y;
       }
-      v[e] = acc;
     }
   } else {
     const int which = blockIdx.y;
-    const T* Wp[MAX_TERMS];
-#pragma unroll
-    for (int n = 0; n < MAX_TERMS; n++) Wp[n] = pall + (size_t)a.w_idx[n < a.L + 1 ? n : 0] * psz + rowoff;
-    const T* pex = pall + (size_t)a.ex * psz + rowoff;
-    const T* pey = pall + (size_t)a.ey * psz + rowoff;
-    const T* ppx = pall + (size_t)a.px * psz + rowoff;
-    const T* ppy = pall + (size_t)a.py * psz + rowoff;
+    const C* pex = reinterpret_cast<const C*>(pall + (size_t)a.ex * psz + rowoff);
+    const C* pey = reinterpret_cast<const C*>(pall + (size_t)a.ey * psz + rowoff);
+    const C* ppx = reinterpret_cast<const C*>(pall + (size_t)a.px * psz + rowoff);
+    const C* ppy = reinterpret_cast<const C*>(pall + (size_t)a.py * psz + rowoff);
+    const int L = a.L;
 #pragma unroll
     for (int e = 0; e < E; e++) {
       const int m = t + e * P;
-      const T r0 = rhs_point<T>(a, Wp, 2 * m, pex[2 * m], pey[2 * m], ppx[2 * m], ppy[2 * m], which);
-      const T r1 = rhs_point<T>(a, Wp, 2 * m + 1, pex[2 * m + 1], pey[2 * m + 1], ppx[2 * m + 1], ppy[2 * m + 1], which);
-      v[e] = mkc(r0, r1);
+      const C ex = pex[m], ey = pey[m], px = ppx[m], py = ppy[m];
+      T W0[MAX_TERMS], W1[MAX_TERMS];
+#pragma unroll
+      for (int n = 0; n < MAX_TERMS; n++) {
+        C w = mkc((T)0, (T)0);
+        if (n <= L) w = reinterpret_cast<const C*>(pall + (size_t)a.w_idx[n] * psz + rowoff)[m];
+        W0[n] = w.x;
+        W1[n] = w.y;
+      }
+      v[e] = mkc(rhs_point<T>(a, W0, ex.x, ey.x, px.x, py.x, which), rhs_point<T>(a, W1, ex.y, ey.y, px.y, py.y, which));
     }
   }
 
@@ -552,7 +552,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yfwd(const __grid_constant__
   // place, one (k, H-k) pair per thread slot
   __syncthreads();
 #pragma unroll
-  for (int e = 0; e < E; e++) tl[spad<E>(t + e * P)] = v[e];
+  for (int e = 0; e < E; e++) tl[(t + e * P)] = v[e];
   __syncthreads();
 #pragma unroll
   for (int e = 0; e <= E / 2; e++) {
@@ -561,8 +561,8 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yfwd(const __grid_constant__
     else if (t == 0) k = H / 2;    // the self-paired middle bin
     else break;
     const int kn = H - k;  // partner; for k = 0 the partner is the Nyquist bin H (C[H] = C[0])
-    const C ck = tl[spad<E>(k)];
-    const C cq = tl[spad<E>(kn & (H - 1))];
+    const C ck = tl[(k)];
+    const C cq = tl[(kn & (H - 1))];
     // X[k] = (C[k] + conj C[H-k])/2 + w^k (C[k] - conj C[H-k])/(2i),  w = exp(-2 pi i / Ny)
     const C cn = cconj(cq);
     const C ev = cscale(cadd(ck, cn), (T)0.5);
@@ -574,16 +574,16 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yfwd(const __grid_constant__
       const C ev2 = cscale(cadd(cq, cm), (T)0.5);
       const C d2 = csub(cq, cm);
       const C od2 = mkc((T)0.5 * d2.y, (T)-0.5 * d2.x);
-      tl[spad<E>(kn)] = cadd(ev2, cmul(__ldg(&twy[kn]), od2));
+      tl[(kn)] = cadd(ev2, cmul(__ldg(&twy[kn]), od2));
     }
-    tl[spad<E>(k)] = xk;
+    tl[(k)] = xk;
   }
   __syncthreads();
   C* vo = reinterpret_cast<C*>(a.vout) + (size_t)blockIdx.y * fsz;
   const int ntot = G * a.rows_out;
   for (int q = threadIdx.x; q < ntot; q += blockDim.x) {
     const int ky = q / G, g = q - ky * G;
-    vo[(size_t)ky * nx + ix0 + g] = sm[(size_t)g * a.lp + spad<E>(ky)];
+    vo[(size_t)ky * nx + ix0 + g] = sm[(size_t)g * a.lp + (ky)];
   }
 }
 

@@ -1,5 +1,5 @@
-// Lookup of the compiled pass-kernel instantiations by precision, mode and
-// line length.
+// Lookup of the compiled pass-kernel instantiations by precision, mode, line
+// length and elements per thread.
 #pragma once
 
 #include "hos_kernels.cuh"
@@ -11,13 +11,16 @@ using XFwdFn = void (*)(XFwdArgs, const void*);
 using YInvFn = void (*)(YInvArgs, const void*, const void*);
 using YFwdFn = void (*)(YFwdArgs, const void*, const void*);
 
-// Elements per thread chosen for a line length (one instantiation per length).
-constexpr int elems_for(int n) { return n <= 8 ? n : (n <= 2048 ? 8 : 16); }
+// Elements per thread a line of length n is compiled for: 8 and 16 (n >= 16),
+// and 32 in single precision (n >= 64); at most MAX_THREADS threads a line.
+constexpr bool elems_valid(int prec, int n, int e) {
+  return (e == 8 || e == 16 || (e == 32 && prec == 1)) && n >= e && n / e <= MAX_THREADS && (e != 32 || n >= 64);
+}
 
-// prec: 0 = double, 1 = float.  Return nullptr for an unsupported length.
-XInvFn lookup_xinv(int prec, int mode, int n);
-XFwdFn lookup_xfwd(int prec, int mode, int n);
-YInvFn lookup_yinv(int prec, int mode, int h);
-YFwdFn lookup_yfwd(int prec, int mode, int h);
+// prec: 0 = double, 1 = float.  Return nullptr for an unsupported combination.
+XInvFn lookup_xinv(int prec, int mode, int n, int e);
+XFwdFn lookup_xfwd(int prec, int mode, int n, int e);
+YInvFn lookup_yinv(int prec, int mode, int h, int e);
+YFwdFn lookup_yfwd(int prec, int mode, int h, int e);
 
 }  // namespace hos
