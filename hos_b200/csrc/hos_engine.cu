@@ -121,6 +121,11 @@ static int fail(int code, const char* fmt, ...) {
   return code;
 }
 
+namespace hos {
+// Lets other translation units of the library report through hos_last_error().
+void set_last_error(const char* msg) { g_err = msg; }
+}  // namespace hos
+
 #define HOS_CK(x)                                                                                  \
   do {                                                                                             \
     cudaError_t e_ = (x);                                                                          \

@@ -137,6 +137,23 @@ int hos_profile_stage(hos_handle h, double dt, int reps, hos_pass_stat* out, int
 /* Kernel launches of this library in one RK step of the handle. */
 int hos_launches_per_step(hos_handle h);
 
+/* The normalised 2-D real-to-complex transform of fft_2d for callers that
+ * cannot allocate GPU memory: code running while a stream is captured into a
+ * CUDA graph (cudaMalloc/cudaFree are not permitted there), latency-critical
+ * loops in which an allocation would synchronise the device, and hosts whose
+ * own allocator owns all device memory.  No counterpart in the reference:
+ * it is this library's addition.  u_phys (real [nx][ny]) and hu (complex
+ * [ny/2+1][nx], interleaved) are device pointers; the transform runs on
+ * `stream` (a cudaStream_t, 0 for the default stream) and nothing is
+ * allocated or freed: the intermediate lives in a fixed device array of the
+ * library (about 8.5 MB per GPU, held until exit).  Limits: nx, ny powers of
+ * two in [16, 2048] and nx*(ny/2+1) <= 525312 (e.g. 1024 x 1024); larger
+ * grids return HOS_ERR_ARG.  The first call on a device looks up that
+ * array's device address and should come before any stream capture.  All
+ * calls on a device share the array, so calls that overlap on the GPU race;
+ * order them on one stream. */
+int hos_fft_2d_noalloc(const double* u_phys, double* hu, int nx, int ny, void* stream);
+
 /* CUDA stream of the handle (a cudaStream_t), for callers that order their
  * own work against it. */
 void* hos_stream(hos_handle h);
