@@ -87,6 +87,11 @@ _SIGNATURES = {
     "hos_clear_history": (_I, [_H]),
     "hos_rhs": (_I, [_H, _P, _P, _D]),
     "hos_fft_2d": (_I, [_H, _P, _P]),
+    "hos_fft_2d_ld": (_I, [_H, _P, _I, _P]),
+    "hos_ifft_2d_ld": (_I, [_H, _P, _P, _I]),
+    "hos_zvel": (_I, [_H, _P, _P, _P, _P, _P]),
+    "hos_spectral_op": (_I, [_H, _I, _P, _P, _P]),
+    "hos_hamiltonian": (_I, [_H, _P, _P, _P, _DP]),
     "hos_ifft_2d": (_I, [_H, _P, _P]),
     "hos_check_finite": (_I, [_H, ctypes.POINTER(_I)]),
     "hos_volume": (_I, [_H, _DP]),

@@ -104,6 +104,74 @@ __global__ void __launch_bounds__(256) k_step_end(const double* ham_part, int np
   *stepdev = st + 1;
 }
 
+// Elementwise spectral operators on one field [h+1][nx] (operators_par.c):
+// 0 Dx (i kx, :20-75), 1 Dy (i ky, :85-120), 2 Dz (|k| or |k| tanh(|k|h), :130-196),
+// 3 Dealias (:283-325), 4 Sum (:247-279).
+__global__ void k_spec_op(Geo g, int op, const double2* a, const double2* b, double2* out) {
+  const size_t n = (size_t)(g.h + 1) * g.nx;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const int row = (int)(q / g.nx), i = (int)(q % g.nx);
+    const double2 x = a[q];
+    double2 r;
+    if (op == 0) {
+      const double kx = kx_of(g, i);
+      r = make_double2(-kx * x.y, kx * x.x);
+    } else if (op == 1) {
+      const double ky = ky_of(g, row);
+      r = make_double2(-ky * x.y, ky * x.x);
+    } else if (op == 2) {
+      const double kx = kx_of(g, i), ky = ky_of(g, row);
+      const double m = dz_mult(g, sqrt(kx * kx + ky * ky), 1);
+      r = make_double2(m * x.x, m * x.y);
+    } else if (op == 3) {
+      r = keep_mode(g, i, row) ? x : make_double2(0.0, 0.0);
+    } else {
+      const double2 y = b[q];
+      r = make_double2(x.x + y.x, x.y + y.y);
+    }
+    out[q] = r;
+  }
+}
+
+__global__ void k_mul_real(const double* a, const double* b, double* out, size_t n) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)
+    out[q] = a[q] * b[q];
+}
+
+// Hamiltonian (hosm_2d_par.c:462-523): one partial per ky row, weight 1 for
+// ky = 0 and 2 otherwise.
+__global__ void __launch_bounds__(256) k_ham_rows(Geo g, const double2* eta, const double2* eta_t, const double2* phi,
+                                                  double* part) {
+  __shared__ double red[256];
+  const int row = blockIdx.x;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < g.nx; i += blockDim.x) {
+    const size_t q = (size_t)row * g.nx + i;
+    const double2 e = eta[q], et = eta_t[q], p = phi[q];
+    s += g.g * e.x * e.x + g.g * e.y * e.y + p.x * et.x + p.y * et.y;
+  }
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[row] = (row == 0 ? 1.0 : 2.0) * red[0];
+}
+
+__global__ void __launch_bounds__(256) k_sum_parts(const double* part, int n, double* out) {
+  __shared__ double red[256];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += part[i];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = red[0];
+}
+
 }  // namespace hos
 
 using namespace hos;
@@ -273,6 +341,8 @@ struct hos_ctx {
   void* phys = nullptr;
   double2* ustage = nullptr;
   double2* ustg = nullptr;  // stage input of the current RK stage
+  double2* zvbuf = nullptr; // Zvel outputs / operator scratch (allocated on first use)
+  double* hpart = nullptr;  // Hamiltonian row partials (allocated on first use)
   double2* zplain = nullptr;
   double* pplain = nullptr;
   void* tw[2][3] = {};  // [precision][nx, ny/2, ny] twiddle tables
@@ -442,8 +512,11 @@ void log_pass(hos_ctx* c, PassLog* lg, int kind, double bytes) {
 }
 
 // Enqueues one RK stage (or one bare RHS evaluation when rhs_only).
+// zvel_out: when set, the stage ends after the W recursion and Zvel's four
+// spectral outputs W^(M), W^(M-2), (W^2)^(M), (W^2)^(M-2) (hosm_2d_par.c:240-445)
+// are written there (4 consecutive FP64 fields) instead of the RHS.
 int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, double2* kout, const double* tsrc,
-                  const int* rows_dev, PassLog* lg = nullptr) {
+                  const int* rows_dev, PassLog* lg = nullptr, double2* zvel_out = nullptr) {
   const PassCfg& g = c->cfg;
   const int M = c->M, L = c->L;
   const size_t fsz = c->fsz;
@@ -529,6 +602,32 @@ int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, dou
     for (int p = 1; p <= n; p++) yl.w_in[p - 1] = c->D(n - p + 1, p + 1);  // power p: m = n - p
     g.yinv[YI_LEVEL]<<<dim3(ygrid(c, g.yi), nl), g.yi.threads, g.yi.smem, c->st>>>(yl, g.twh, g.twy);
     log_pass(c, lg, P_YINV_LEVEL, fszd * (double)cs * (M - n) + psz * (double)rs * (M - n + 1 + n + 1));
+  }
+
+  if (zvel_out) {
+    YFwdArgs zf{};
+    zf.geo = c->geo;
+    zf.lp = g.yf.lp;
+    zf.phys = c->phys;
+    zf.ex = c->ETAX();
+    zf.ey = c->ETAY();
+    zf.px = c->PHIX();
+    zf.py = c->PHIY();
+    zf.L = L;
+    for (int n = 0; n <= L; n++) zf.w_idx[n] = c->W(n);
+    zf.which_base = 2;
+    zf.vout = zb;
+    zf.rows_out = c->h + 1;
+    g.yfwd[YF_RHS]<<<dim3(ygrid(c, g.yf), 4), g.yf.threads, g.yf.smem, c->st>>>(zf, g.twh, g.twy);
+    XFwdArgs xz{};
+    xz.geo = c->geo;
+    xz.rows = c->h + 1;
+    xz.vin0 = zb;
+    xz.out_spec = zvel_out;
+    xz.addk_mask = 1 | (L >= 2 ? 2 : 0);  // W^(1) belongs to W^(M) always and to W^(M-2) when L >= 2
+    xz.u_add = uin;
+    g.xfwd[XF_PLAIN]<<<dim3(xgrid(c, g.xf), 4), g.xf.threads, g.xf.smem, c->st>>>(xz, g.twx);
+    return HOS_OK;
   }
 
   YFwdArgs ff{};
@@ -665,7 +764,7 @@ void release(hos_ctx* c) {
   if (c->graph) cudaGraphDestroy(c->graph);
   void* ptrs[] = {c->u,    c->k,    c->zbuf,    c->phys,   c->ustage, c->ustg, c->zplain,   c->pplain,
                   c->tdev, c->trhs, c->rdev,    c->stepdev, c->actdev, c->flagdev, c->ham_part,
-                  c->ham_hist, c->t_hist, c->tw[0][0], c->tw[0][1], c->tw[0][2], c->tw[1][0], c->tw[1][1], c->tw[1][2]};
+                  c->ham_hist, c->t_hist, c->zvbuf, c->hpart, c->tw[0][0], c->tw[0][1], c->tw[0][2], c->tw[1][0], c->tw[1][1], c->tw[1][2]};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->st) cudaStreamDestroy(c->st);
@@ -832,6 +931,7 @@ int hos_create(const hos_params* p, hos_handle* out) {
   if (e == cudaSuccess) e = cudaMemsetAsync(c->u, 0, 2 * c->fsz * sizeof(double2), c->st);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->k, 0, (size_t)c->nst * 2 * c->fsz * sizeof(double2), c->st);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->tdev, 0, sizeof(double), c->st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->trhs, 0, sizeof(double), c->st);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->stepdev, 0, sizeof(long long), c->st);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->ham_part, 0, (size_t)c->nparts * sizeof(double), c->st);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->ham_hist, 0, HIST_CAP * sizeof(double), c->st);
@@ -976,6 +1076,28 @@ int hos_rhs(hos_handle h, const double* u, double* rhs, double t) {
   return HOS_OK;
 }
 
+int hos_fft_2d_ld(hos_handle h, const double* u_phys, int ld, double* hu) {
+  if (!h || !u_phys || !hu || ld < h->ny) return fail(HOS_ERR_ARG, "bad argument");
+  HOS_CK(cudaMemcpy2DAsync(h->pplain, h->ny * sizeof(double), u_phys, (size_t)ld * sizeof(double),
+                           h->ny * sizeof(double), h->nx, cudaMemcpyDefault, h->st));
+  enqueue_r2c(h, h->pplain, h->ustage, 0);
+  HOS_CK(cudaGetLastError());
+  HOS_CK(cudaMemcpyAsync(hu, h->ustage, h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+  HOS_CK(cudaStreamSynchronize(h->st));
+  return HOS_OK;
+}
+
+int hos_ifft_2d_ld(hos_handle h, const double* hu, double* u_phys, int ld) {
+  if (!h || !hu || !u_phys || ld < h->ny) return fail(HOS_ERR_ARG, "bad argument");
+  HOS_CK(cudaMemcpyAsync(h->ustage, hu, h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+  enqueue_c2r(h, h->ustage, h->pplain);
+  HOS_CK(cudaGetLastError());
+  HOS_CK(cudaMemcpy2DAsync(u_phys, (size_t)ld * sizeof(double), h->pplain, h->ny * sizeof(double),
+                           h->ny * sizeof(double), h->nx, cudaMemcpyDefault, h->st));
+  HOS_CK(cudaStreamSynchronize(h->st));
+  return HOS_OK;
+}
+
 int hos_fft_2d(hos_handle h, const double* u_phys, double* hu) {
   if (!h || !u_phys || !hu) return fail(HOS_ERR_ARG, "null argument");
   HOS_CK(cudaMemcpyAsync(h->pplain, u_phys, h->psz * sizeof(double), cudaMemcpyDefault, h->st));
@@ -1050,6 +1172,72 @@ int hos_profile_stage(hos_handle h, double dt, int reps, hos_pass_stat* out, int
   }
   *count = c;
   HOS_CK(cudaGetLastError());
+  return HOS_OK;
+}
+
+int hos_zvel(hos_handle h, const double* u, double* wM, double* wM2, double* w2M, double* w2M2) {
+  if (!h || !u || !wM || !wM2 || !w2M || !w2M2) return fail(HOS_ERR_ARG, "null argument");
+  if (!h->zvbuf) {
+    int rc = dalloc(&h->zvbuf, 4 * h->fsz * sizeof(double2));
+    if (rc) return rc;
+  }
+  HOS_CK(cudaMemcpyAsync(h->ustage, u, 2 * h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+  int rc = enqueue_stage(h, 0, 0.0, true, h->ustage, nullptr, h->trhs, nullptr, nullptr, h->zvbuf);
+  if (rc) return rc;
+  HOS_CK(cudaGetLastError());
+  double* outs[4] = {wM, wM2, w2M, w2M2};
+  for (int q = 0; q < 4; q++)
+    HOS_CK(cudaMemcpyAsync(outs[q], h->zvbuf + (size_t)q * h->fsz, h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+  HOS_CK(cudaStreamSynchronize(h->st));
+  return HOS_OK;
+}
+
+int hos_spectral_op(hos_handle h, int op, const double* a, const double* b, double* out) {
+  if (!h || !a || !out || ((op == HOS_OP_SUM || op == HOS_OP_MULT) && !b)) return fail(HOS_ERR_ARG, "null argument");
+  if (op < HOS_OP_DX || op > HOS_OP_MULT) return fail(HOS_ERR_ARG, "unknown operator %d", op);
+  if (!h->zvbuf) {
+    int rc = dalloc(&h->zvbuf, 4 * h->fsz * sizeof(double2));
+    if (rc) return rc;
+  }
+  double2* da = h->zvbuf;
+  double2* db = h->zvbuf + h->fsz;
+  double2* dout = h->zvbuf + 2 * h->fsz;
+  HOS_CK(cudaMemcpyAsync(da, a, h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+  if (b) HOS_CK(cudaMemcpyAsync(db, b, h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+  if (op == HOS_OP_MULT) {  // Mult, operators_par.c:210-235
+    enqueue_c2r(h, da, h->pplain);
+    enqueue_c2r(h, db, h->pplain + h->psz);
+    k_mul_real<<<296, 256, 0, h->st>>>(h->pplain, h->pplain + h->psz, h->pplain, h->psz);
+    enqueue_r2c(h, h->pplain, dout, 0);
+  } else {
+    k_spec_op<<<296, 256, 0, h->st>>>(h->geo, op, da, db, dout);
+  }
+  HOS_CK(cudaGetLastError());
+  HOS_CK(cudaMemcpyAsync(out, dout, h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+  HOS_CK(cudaStreamSynchronize(h->st));
+  return HOS_OK;
+}
+
+int hos_hamiltonian(hos_handle h, const double* eta, const double* eta_t, const double* phi, double* H) {
+  if (!h || !eta || !eta_t || !phi || !H) return fail(HOS_ERR_ARG, "null argument");
+  if (!h->zvbuf) {
+    int rc = dalloc(&h->zvbuf, 4 * h->fsz * sizeof(double2));
+    if (rc) return rc;
+  }
+  if (!h->hpart) {
+    int rc = dalloc(&h->hpart, (size_t)(h->h + 2) * sizeof(double));
+    if (rc) return rc;
+  }
+  const double* src[3] = {eta, eta_t, phi};
+  for (int q = 0; q < 3; q++)
+    HOS_CK(cudaMemcpyAsync(h->zvbuf + (size_t)q * h->fsz, src[q], h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+  k_ham_rows<<<h->h + 1, 256, 0, h->st>>>(h->geo, h->zvbuf, h->zvbuf + h->fsz, h->zvbuf + 2 * h->fsz, h->hpart);
+  k_sum_parts<<<1, 256, 0, h->st>>>(h->hpart, h->h + 1, h->hpart + h->h + 1);
+  HOS_CK(cudaGetLastError());
+  double r = 0.0;
+  HOS_CK(cudaMemcpyAsync(&r, h->hpart + h->h + 1, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  HOS_CK(cudaStreamSynchronize(h->st));
+  *H = r;
   return HOS_OK;
 }
 

@@ -164,8 +164,10 @@ struct XFwdArgs {
   int rows_fft;         // RHS: rows < rows_fft are transformed; rows in [rows_fft, rows) only add to the Hamiltonian
   const void* vin0;     // input V arrays (T2) [h+1][nx]; RHS: blockIdx.y selects vin0 (eta) or vin1 (phi)
   const void* vin1;
-  double2* out_spec;    // PLAIN output
+  double2* out_spec;    // PLAIN output; blockIdx.y = q reads vin0 + q*fsz and writes out_spec + q*fsz
   int dealias;          // PLAIN: zero the modes Dealias zeroes (operators_par.c:283-325)
+  int addk_mask;        // PLAIN: bit q set -> add Dz of the phi field of u_add to output q (W^(1), hosm_2d_par.c:280-288)
+  const double2* u_add; // PLAIN: packed state whose phi field supplies that term
   void* zout;           // LEVEL: output Z arrays (T2), stride (h+1)*nx; order blockIdx.y+1
   // RHS
   double2* u;                     // packed state at step start (updated in place on the final stage)
@@ -200,7 +202,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_xfwd(const __grid_constant__
     const T sc = (T)geo.inv_nxny;
     const bool live = row < a.rows;
     const size_t roff = (size_t)(live ? row : 0) * NX;
-    const C* vin = reinterpret_cast<const C*>(a.vin0);
+    const C* vin = reinterpret_cast<const C*>(a.vin0) + (MODE == XF_PLAIN ? (size_t)blockIdx.y * fsz : 0);
     C v[E];
 #pragma unroll
     for (int e = 0; e < E; e++) v[e] = live ? vin[roff + t + e * P] : mkc((T)0, (T)0);
@@ -209,10 +211,22 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_xfwd(const __grid_constant__
     for (int e = 0; e < E; e++) v[e] = cscale(v[e], sc);  // fft_2d's 1/Nx/Ny (exact: powers of two)
     if (MODE == XF_PLAIN) {
       if (live) {
+        double2* out = a.out_spec + (size_t)blockIdx.y * fsz;
+        const bool addk = (a.addk_mask >> blockIdx.y) & 1;
+        const double ky = ky_of(geo, row);
 #pragma unroll
         for (int e = 0; e < E; e++) {
-          const bool z0 = a.dealias && !keep_mode(geo, t + e * P, row);
-          a.out_spec[roff + t + e * P] = z0 ? make_double2(0.0, 0.0) : widen(v[e]);
+          const int i = t + e * P;
+          const bool z0 = a.dealias && !keep_mode(geo, i, row);
+          double2 r = z0 ? make_double2(0.0, 0.0) : widen(v[e]);
+          if (addk) {
+            const double kx = kx_of(geo, i);
+            const double m1 = dz_mult(geo, sqrt(kx * kx + ky * ky), 1);
+            const double2 ph = a.u_add[fsz + roff + i];
+            r.x += m1 * ph.x;
+            r.y += m1 * ph.y;
+          }
+          out[roff + i] = r;
         }
       }
       return;
@@ -441,15 +455,26 @@ struct YFwdArgs {
   int ex, ey, px, py;
   int L;
   int w_idx[MAX_TERMS];  // W_0..W_L
+  int which_base;        // RHS: output blockIdx.y computes quantity which_base + blockIdx.y
   void* vout;            // output V arrays (T2), stride (h+1)*nx; output = blockIdx.y
   int rows_out;
 };
 
-// RHS assembly at one physical point: P_eta (which = 0) or P_phi (which = 1).
+// RHS assembly at one physical point: P_eta (which = 0) or P_phi (which = 1);
+// which = 2..5 give the physical parts of Zvel's outputs: W^(M) and W^(M-2)
+// without W^(1) (which is added in spectral space), (W^2)^(M), (W^2)^(M-2)
+// (hosm_2d_par.c:362-442).
 template <typename T>
 __device__ __forceinline__ T rhs_point(const YFwdArgs& a, const T* W, T ex, T ey, T px, T py, int which) {
   const int L = a.L;
   const T grad2 = ex * ex + ey * ey;
+  if (which == 2 || which == 3) {
+    T s = (T)0;
+#pragma unroll
+    for (int n = 1; n < MAX_TERMS; n++)
+      if (n <= (which == 2 ? L : L - 2)) s += W[n];
+    return s;
+  }
   if (which == 0) {
     T s1 = (T)0, wm2 = (T)0;
 #pragma unroll
@@ -471,6 +496,8 @@ __device__ __forceinline__ T rhs_point(const YFwdArgs& a, const T* W, T ex, T ey
     else w2m += s;
   }
   w2m += w2m2;
+  if (which == 4) return w2m;
+  if (which == 5) return w2m2;
   return (T)0.5 * (w2m + grad2 * w2m2) - (T)0.5 * (px * px + py * py);  // hosm_2d_par.c:181-206
 }
 
@@ -525,7 +552,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yfwd(const __grid_constant__
       }
     }
   } else {
-    const int which = blockIdx.y;
+    const int which = blockIdx.y + a.which_base;
     const C* pex = reinterpret_cast<const C*>(pall + (size_t)a.ex * psz + rowoff);
     const C* pey = reinterpret_cast<const C*>(pall + (size_t)a.ey * psz + rowoff);
     const C* ppx = reinterpret_cast<const C*>(pall + (size_t)a.px * psz + rowoff);

@@ -173,6 +173,28 @@ class HosField:
         _lib.check(self._lib.hos_rhs(self._h, _ptr(a), _ptr(out), float(t)))
         return out
 
+    def zvel(self, u):
+        """Zvel (hosm_2d_par.c:240-445): spectral W^(M), W^(M-2), (W^2)^(M), (W^2)^(M-2)."""
+        a = self._as_spec(u, 2)
+        outs = [self._spec(1) for _ in range(4)]
+        _lib.check(self._lib.hos_zvel(self._h, _ptr(a), *[_ptr(o) for o in outs]))
+        return outs
+
+    def spectral_op(self, op, a, b=None):
+        """Dx, Dy, Dz, Dealias, Sum, Mult of operators_par.c on one field."""
+        codes = {"Dx": 0, "Dy": 1, "Dz": 2, "Dealias": 3, "Sum": 4, "Mult": 5}
+        x = self._as_spec(a, 1)
+        y = self._as_spec(b, 1) if b is not None else None
+        out = self._spec(1)
+        _lib.check(self._lib.hos_spectral_op(self._h, codes[op], _ptr(x), _ptr(y) if y is not None else None, _ptr(out)))
+        return out
+
+    def hamiltonian(self, heta, heta_t, hphi):
+        a, b, c = (self._as_spec(x, 1) for x in (heta, heta_t, hphi))
+        H = ctypes.c_double()
+        _lib.check(self._lib.hos_hamiltonian(self._h, _ptr(a), _ptr(b), _ptr(c), ctypes.byref(H)))
+        return H.value
+
     def fft_2d(self, x):
         a = self._as_phys(x)
         out = self._spec(1)

@@ -114,6 +114,24 @@ int hos_rhs(hos_handle h, const double* u, double* rhs, double t);
  * normalised r2c of a physical field and unnormalised c2r of a spectral one. */
 int hos_fft_2d(hos_handle h, const double* u_phys, double* hu);
 int hos_ifft_2d(hos_handle h, const double* hu, double* u_phys);
+/* The same with a physical row stride of ld >= ny doubles (the reference's
+ * padded layout has ld = ny + 2, fft_routines_2d_par.c:19,86). */
+int hos_fft_2d_ld(hos_handle h, const double* u_phys, int ld, double* hu);
+int hos_ifft_2d_ld(hos_handle h, const double* hu, double* u_phys, int ld);
+
+/* Zvel (hosm_2d_par.c:240-445) on a packed spectral state: the spectral
+ * W^(M), W^(M-2), (W^2)^(M), (W^2)^(M-2), each one field [ny/2+1][nx]. */
+int hos_zvel(hos_handle h, const double* u, double* wM, double* wM2, double* w2M, double* w2M2);
+
+/* The spectral operators of operators_par.c on one field [ny/2+1][nx]:
+ * Dx (:20-75), Dy (:85-120), Dz (:130-196; |k| tanh(|k|h) for finite
+ * depth), Dealias (:283-325), Sum (:247-279, uses b) and Mult (:210-235,
+ * uses b: c2r both, multiply, normalised r2c). */
+enum { HOS_OP_DX = 0, HOS_OP_DY = 1, HOS_OP_DZ = 2, HOS_OP_DEALIAS = 3, HOS_OP_SUM = 4, HOS_OP_MULT = 5 };
+int hos_spectral_op(hos_handle h, int op, const double* a, const double* b, double* out);
+
+/* Hamiltonian (hosm_2d_par.c:462-523) of spectral eta, eta_t, phi. */
+int hos_hamiltonian(hos_handle h, const double* eta, const double* eta_t, const double* phi, double* H);
 
 /* Whether the resident state is finite (1) or holds NaN/Inf (0). */
 int hos_check_finite(hos_handle h, int* finite);

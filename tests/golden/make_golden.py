@@ -79,6 +79,15 @@ def main():
         save(f"rhs_m{M}_{nx}x{ny}_{'d' if dealias else 'nd'}_r{ramp}", u=u, rhs=r, t=0.7,
              meta=np.array([nx, ny, M, ramp]), g=9.81 if M == 5 else 1.0, tramp=2.0)
 
+    # 3b. Zvel outputs on random states
+    for (M, nx, ny, seed) in [(4, 32, 32, 31), (3, 16, 32, 32), (6, 32, 16, 33)]:
+        rng = np.random.default_rng(seed)
+        hn = HosNumpy(nx, ny, 2 * math.pi, 2 * math.pi, 1.0, M)
+        u = rand_state(rng, nx, ny, 0.01, hn if seed != 32 else None)
+        ref = RefC(M, nx, ny)
+        wM, wM2, w2M, w2M2 = ref.zvel(u)
+        save(f"zvel_m{M}_{nx}x{ny}", u=u, wM=wM, wM2=wM2, w2M=w2M, w2M2=w2M2, meta=np.array([nx, ny, M]))
+
     # 4. each RK scheme, 5 steps on a small JONSWAP sea, M=4
     nx = ny = 32
     eta, phi, info = ic.jonswap(nx, ny, kp=4.0, steepness=0.1, seed=21)
