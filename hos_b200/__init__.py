@@ -7,6 +7,7 @@ is the Python host side: a ctypes binding (``_lib``), the field handle
 """
 from . import ic
 from ._lib import HosError, load
+from .ensemble import HosEnsemble
 from .field import HosField
 
-__all__ = ["HosField", "HosError", "ic", "load"]
+__all__ = ["HosField", "HosEnsemble", "HosError", "ic", "load"]

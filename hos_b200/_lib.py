@@ -98,6 +98,11 @@ _SIGNATURES = {
     "hos_stream": (_P, [_H]),
     "hos_profile_stage": (_I, [_H, _D, _I, ctypes.POINTER(HosPassStat), _I, ctypes.POINTER(_I)]),
     "hos_launches_per_step": (_I, [_H]),
+    "hos_ensemble_create": (_I, [ctypes.POINTER(_H), ctypes.POINTER(_D), _I, ctypes.POINTER(_H)]),
+    "hos_ensemble_step": (_I, [_H, _I]),
+    "hos_ensemble_sync": (_I, [_H]),
+    "hos_ensemble_info": (_I, [_H, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "hos_ensemble_destroy": (_I, [_H]),
     "hos_last_error": (ctypes.c_char_p, []),
     "hos_version": (ctypes.c_char_p, []),
 }

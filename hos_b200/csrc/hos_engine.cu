@@ -23,31 +23,32 @@
 #include <cstdlib>
 #include <mutex>
 #include <string>
+#include <algorithm>
 #include <vector>
 
 #include "hos_gpu.h"
 #include "hos_registry.h"
 
 namespace hos {
-XInvFn lookup_xinv_64(int mode, int n, int e);
-XFwdFn lookup_xfwd_64(int mode, int n, int e);
-YInvFn lookup_yinv_64(int mode, int h, int e);
-YFwdFn lookup_yfwd_64(int mode, int h, int e);
-XInvFn lookup_xinv_32(int mode, int n, int e);
-XFwdFn lookup_xfwd_32(int mode, int n, int e);
-YInvFn lookup_yinv_32(int mode, int h, int e);
-YFwdFn lookup_yfwd_32(int mode, int h, int e);
-XInvFn lookup_xinv(int prec, int mode, int n, int e) {
-  return prec ? lookup_xinv_32(mode, n, e) : lookup_xinv_64(mode, n, e);
+XInvFn lookup_xinv_64(int mode, int n, int e, bool batch);
+XFwdFn lookup_xfwd_64(int mode, int n, int e, bool batch);
+YInvFn lookup_yinv_64(int mode, int h, int e, bool batch);
+YFwdFn lookup_yfwd_64(int mode, int h, int e, bool batch);
+XInvFn lookup_xinv_32(int mode, int n, int e, bool batch);
+XFwdFn lookup_xfwd_32(int mode, int n, int e, bool batch);
+YInvFn lookup_yinv_32(int mode, int h, int e, bool batch);
+YFwdFn lookup_yfwd_32(int mode, int h, int e, bool batch);
+XInvFn lookup_xinv(int prec, int mode, int n, int e, bool batch) {
+  return prec ? lookup_xinv_32(mode, n, e, batch) : lookup_xinv_64(mode, n, e, batch);
 }
-XFwdFn lookup_xfwd(int prec, int mode, int n, int e) {
-  return prec ? lookup_xfwd_32(mode, n, e) : lookup_xfwd_64(mode, n, e);
+XFwdFn lookup_xfwd(int prec, int mode, int n, int e, bool batch) {
+  return prec ? lookup_xfwd_32(mode, n, e, batch) : lookup_xfwd_64(mode, n, e, batch);
 }
-YInvFn lookup_yinv(int prec, int mode, int h, int e) {
-  return prec ? lookup_yinv_32(mode, h, e) : lookup_yinv_64(mode, h, e);
+YInvFn lookup_yinv(int prec, int mode, int h, int e, bool batch) {
+  return prec ? lookup_yinv_32(mode, h, e, batch) : lookup_yinv_64(mode, h, e, batch);
 }
-YFwdFn lookup_yfwd(int prec, int mode, int h, int e) {
-  return prec ? lookup_yfwd_32(mode, h, e) : lookup_yfwd_64(mode, h, e);
+YFwdFn lookup_yfwd(int prec, int mode, int h, int e, bool batch) {
+  return prec ? lookup_yfwd_32(mode, h, e, batch) : lookup_yfwd_64(mode, h, e, batch);
 }
 
 // ---------------------------------------------------------------- small kernels
@@ -83,8 +84,33 @@ __global__ void k_nonfinite(const double2* u, size_t n, int* flag) {
 // Sums the stage-0 Hamiltonian partials in a fixed order (one block, fixed
 // strides, fixed tree), records (t, H) and advances t
 // (time_schemes_par.c:73-93,119).
+struct StepEndArgs {
+  const double* ham_part;
+  int nparts;
+  double* tdev;
+  double dt;
+  long long* stepdev;
+  double* ham_hist;
+  double* t_hist;
+  int hist_cap;
+};
+
+__device__ void step_end_body(const double* ham_part, int nparts, double* tdev, double dt, long long* stepdev,
+                              double* ham_hist, double* t_hist, int hist_cap);
+
 __global__ void __launch_bounds__(256) k_step_end(const double* ham_part, int nparts, double* tdev, double dt,
                                                   long long* stepdev, double* ham_hist, double* t_hist, int hist_cap) {
+  step_end_body(ham_part, nparts, tdev, dt, stepdev, ham_hist, t_hist, hist_cap);
+}
+
+// One block per ensemble member.
+__global__ void __launch_bounds__(256) k_step_end_b(const StepEndArgs* __restrict__ arr) {
+  const StepEndArgs& a = arr[blockIdx.x];
+  step_end_body(a.ham_part, a.nparts, a.tdev, a.dt, a.stepdev, a.ham_hist, a.t_hist, a.hist_cap);
+}
+
+__device__ void step_end_body(const double* ham_part, int nparts, double* tdev, double dt, long long* stepdev,
+                              double* ham_hist, double* t_hist, int hist_cap) {
   __shared__ double red[256];
   double s = 0.0;
   for (int i = threadIdx.x; i < nparts; i += blockDim.x) s += ham_part[i];
@@ -207,6 +233,12 @@ void set_last_error(const char* msg) { g_err = msg; }
 // ---------------------------------------------------------------- plan
 namespace {
 
+// Elements per thread of each pass kind (x-inverse, x-forward, y-inverse,
+// y-forward); defaults, overridable per handle by the autotuner.
+struct ElemChoice {
+  int xi = 8, xf = 8, yi = 8, yf = 8;
+};
+
 // Launch geometry of one pass kind: elements per thread E, lines per block,
 // threads, dynamic shared memory and (y-passes) the line pitch.
 struct KindCfg {
@@ -220,17 +252,18 @@ struct PassCfg {
   XFwdFn xfwd[3] = {};
   YInvFn yinv[2] = {};
   YFwdFn yfwd[3] = {};
+  XInvFn xinv_b[2] = {};  // batched variants (per-field arguments from a device array)
+  XFwdFn xfwd_b[3] = {};
+  YInvFn yinv_b[2] = {};
+  YFwdFn yfwd_b[3] = {};
+  ElemChoice ec;
   KindCfg xi, xf, yi, yf;
   const void* twx = nullptr;  // length nx
   const void* twh = nullptr;  // length ny/2
   const void* twy = nullptr;  // length ny
 };
 
-// Elements per thread of each pass kind (x-inverse, x-forward, y-inverse,
-// y-forward); defaults, overridable per handle by the autotuner.
-struct ElemChoice {
-  int xi = 8, xf = 8, yi = 8, yf = 8;
-};
+
 
 int ilog2i(int n) {
   int r = 0;
@@ -448,6 +481,11 @@ int make_cfg(hos_ctx* c, int prec, const ElemChoice& ec, PassCfg* o) {
   for (int m = 0; m < 3; m++)
     if (!o->xfwd[m] || !o->yfwd[m] || (m < 2 && (!o->xinv[m] || !o->yinv[m])))
       return fail(HOS_ERR_ARG, "no kernels for %dx%d (E %d/%d/%d/%d)", c->nx, c->ny, exi, exf, eyi, eyf);
+  for (int m = 0; m < 2; m++) o->xinv_b[m] = lookup_xinv(prec, m, c->nx, exi, true);
+  for (int m = 0; m < 3; m++) o->xfwd_b[m] = lookup_xfwd(prec, m, c->nx, exf, true);
+  for (int m = 0; m < 2; m++) o->yinv_b[m] = lookup_yinv(prec, m, c->h, eyi, true);
+  for (int m = 0; m < 3; m++) o->yfwd_b[m] = lookup_yfwd(prec, m, c->h, eyf, true);
+  o->ec = ec;
   if (x_geometry(c->nx, exi, cs, &o->xi) || x_geometry(c->nx, exf, cs, &o->xf) ||
       y_geometry(c->h, c->nx, eyi, cs, &o->yi) || y_geometry(c->h, c->nx, eyf, cs, &o->yf))
     return fail(HOS_ERR_ARG, "no launch geometry for %dx%d", c->nx, c->ny);
@@ -459,6 +497,13 @@ int make_cfg(hos_ctx* c, int prec, const ElemChoice& ec, PassCfg* o) {
     HOS_CK(cudaFuncSetAttribute((const void*)o->yinv[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->yi.smem));
   for (int m = 0; m < 3; m++)
     HOS_CK(cudaFuncSetAttribute((const void*)o->yfwd[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->yf.smem));
+  auto setb = [](const void* f, size_t smem) -> cudaError_t {
+    return f ? cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) : cudaSuccess;
+  };
+  for (int m = 0; m < 2; m++) HOS_CK(setb((const void*)o->xinv_b[m], o->xi.smem));
+  for (int m = 0; m < 3; m++) HOS_CK(setb((const void*)o->xfwd_b[m], o->xf.smem));
+  for (int m = 0; m < 2; m++) HOS_CK(setb((const void*)o->yinv_b[m], o->yi.smem));
+  for (int m = 0; m < 3; m++) HOS_CK(setb((const void*)o->yfwd_b[m], o->yf.smem));
   o->twx = c->tw[prec][0];
   o->twh = c->tw[prec][1];
   o->twy = c->tw[prec][2];
@@ -511,23 +556,46 @@ void log_pass(hos_ctx* c, PassLog* lg, int kind, double bytes) {
   lg->bytes.push_back(bytes);
 }
 
-// Enqueues one RK stage (or one bare RHS evaluation when rhs_only).
+// One pass launch of a stage: which kernel, its grid and its arguments.  A
+// stage is built as a list of these; one field launches them by value, an
+// ensemble gathers the arguments of many fields into device arrays and
+// launches each pass once per size class (blockIdx.z = field).
+enum LaunchKind { L_XINV, L_XFWD, L_YINV, L_YFWD };
+struct PassRec {
+  int kind = 0, mode = 0;
+  int gx = 1, gy = 1;  // grid (x: rows or x-row groups, y: outputs)
+  int log_kind = 0;    // PassKind for the per-pass profile
+  double bytes = 0.0;  // algorithmic bytes of the launch
+  XInvArgs xi{};
+  XFwdArgs xf{};
+  YInvArgs yi{};
+  YFwdArgs yf{};
+};
+
+// Builds one RK stage (or one bare RHS evaluation when rhs_only).
 // zvel_out: when set, the stage ends after the W recursion and Zvel's four
 // spectral outputs W^(M), W^(M-2), (W^2)^(M), (W^2)^(M-2) (hosm_2d_par.c:240-445)
 // are written there (4 consecutive FP64 fields) instead of the RHS.
-int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, double2* kout, const double* tsrc,
-                  const int* rows_dev, PassLog* lg = nullptr, double2* zvel_out = nullptr) {
+// act_rows is only used for the byte counts of the profile.
+void build_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, double2* kout, const double* tsrc,
+                 const int* rows_dev, double2* zvel_out, int act_rows, std::vector<PassRec>& out) {
   const PassCfg& g = c->cfg;
   const int M = c->M, L = c->L;
   const size_t fsz = c->fsz;
   const size_t cs = c->prec ? sizeof(float2) : sizeof(double2);
   const size_t rs = c->prec ? sizeof(float) : sizeof(double);
   char* zb = reinterpret_cast<char*>(c->zbuf);
-  const double act = lg ? (double)lg->act_rows : 0.0;
+  const double act = (double)act_rows;
   const double nxd = (double)c->nx, psz = (double)c->psz, fszd = (double)fsz, my = (double)c->geo.my;
 
-  XInvArgs xa{};
+  PassRec r1;
+  r1.kind = L_XINV;
+  r1.mode = XI_STAGE;
+  r1.gx = xgrid(c, g.xi);
+  r1.gy = 4 + M;
+  XInvArgs& xa = r1.xi;
   xa.geo = c->geo;
+  xa.ycount = 4 + M;
   xa.rows = c->h + 1;
   xa.rows_dev = rows_dev;
   xa.u = uin;
@@ -547,10 +615,15 @@ int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, dou
   xa.set_ramp = (s == 0);
   xa.tramp = c->p.tramp;
   xa.rampflg = c->p.rampflg;
-  g.xinv[XI_STAGE]<<<dim3(xgrid(c, g.xi), 4 + M), g.xi.threads, g.xi.smem, c->st>>>(xa, g.twx);
-  log_pass(c, lg, P_XINV_STAGE, act * nxd * (16.0 * 2 * (1 + nk) + (double)cs * (4 + M)));
+  r1.log_kind = P_XINV_STAGE;
+  r1.bytes = act * nxd * (16.0 * 2 * (1 + nk) + (double)cs * (4 + M));
+  out.push_back(r1);
 
-  YInvArgs ya{};
+  PassRec r2;
+  r2.kind = L_YINV;
+  r2.mode = YI_JOBS;
+  r2.gx = ygrid(c, g.yi);
+  YInvArgs& ya = r2.yi;
   ya.geo = c->geo;
   ya.lp = g.yi.lp;
   ya.z = c->zbuf;
@@ -564,12 +637,21 @@ int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, dou
   ya.jobs[nj++] = YJob{2, 1, c->PHIY()};
   ya.jobs[nj++] = YJob{3, 0, c->PHIX()};
   for (int j = 1; j <= M; j++) ya.jobs[nj++] = YJob{4 + j - 1, 0, c->D(1, j)};
-  g.yinv[YI_JOBS]<<<dim3(ygrid(c, g.yi), nj), g.yi.threads, g.yi.smem, c->st>>>(ya, g.twh, g.twy);
-  log_pass(c, lg, P_YINV_STAGE, act * nxd * (double)cs * (4 + M) + psz * (double)rs * (5 + M));
+  ya.ycount = nj;
+  r2.gy = nj;
+  r2.log_kind = P_YINV_STAGE;
+  r2.bytes = act * nxd * (double)cs * (4 + M) + psz * (double)rs * (5 + M);
+  out.push_back(r2);
 
   for (int n = 1; n <= L; n++) {
-    YFwdArgs fa{};
+    PassRec r3;
+    r3.kind = L_YFWD;
+    r3.mode = YF_LEVEL;
+    r3.gx = ygrid(c, g.yf);
+    r3.gy = 1;
+    YFwdArgs& fa = r3.yf;
     fa.geo = c->geo;
+    fa.ycount = 1;
     fa.lp = g.yf.lp;
     fa.phys = c->phys;
     fa.eta = c->ETA();
@@ -577,18 +659,30 @@ int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, dou
     for (int p = 1; p <= n; p++) fa.t_in[p - 1] = c->D(n - p + 1, p);  // power p: m = n - p
     fa.vout = zb;
     fa.rows_out = c->h + 1;
-    g.yfwd[YF_LEVEL]<<<dim3(ygrid(c, g.yf), 1), g.yf.threads, g.yf.smem, c->st>>>(fa, g.twh, g.twy);
-    log_pass(c, lg, P_YFWD_LEVEL, psz * (double)rs * (n + 1) + fszd * (double)cs);
+    r3.log_kind = P_YFWD_LEVEL;
+    r3.bytes = psz * (double)rs * (n + 1) + fszd * (double)cs;
+    out.push_back(r3);
 
-    XFwdArgs xf{};
+    PassRec r4;
+    r4.kind = L_XFWD;
+    r4.mode = XF_LEVEL;
+    r4.gx = xgrid(c, g.xf);
+    r4.gy = M - n;
+    XFwdArgs& xf = r4.xf;
     xf.geo = c->geo;
+    xf.ycount = M - n;
     xf.rows = c->h + 1;
     xf.vin0 = zb;
     xf.zout = zb + fsz * cs;
-    g.xfwd[XF_LEVEL]<<<dim3(xgrid(c, g.xf), M - n), g.xf.threads, g.xf.smem, c->st>>>(xf, g.twx);
-    log_pass(c, lg, P_XFWD_LEVEL, fszd * (double)cs * (1 + M - n));
+    r4.log_kind = P_XFWD_LEVEL;
+    r4.bytes = fszd * (double)cs * (1 + M - n);
+    out.push_back(r4);
 
-    YInvArgs yl{};
+    PassRec r5;
+    r5.kind = L_YINV;
+    r5.mode = YI_LEVEL;
+    r5.gx = ygrid(c, g.yi);
+    YInvArgs& yl = r5.yi;
     yl.geo = c->geo;
     yl.lp = g.yi.lp;
     yl.z = c->zbuf;
@@ -596,17 +690,26 @@ int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, dou
     yl.phys = c->phys;
     int nl = 0;
     for (int j = 1; j <= M - n; j++) yl.jobs[nl++] = YJob{1 + j - 1, 0, c->D(n + 1, j)};
+    yl.ycount = nl;
+    r5.gy = nl;
     yl.w_out = c->W(n);
     yl.eta = c->ETA();
     yl.w_terms = n;
     for (int p = 1; p <= n; p++) yl.w_in[p - 1] = c->D(n - p + 1, p + 1);  // power p: m = n - p
-    g.yinv[YI_LEVEL]<<<dim3(ygrid(c, g.yi), nl), g.yi.threads, g.yi.smem, c->st>>>(yl, g.twh, g.twy);
-    log_pass(c, lg, P_YINV_LEVEL, fszd * (double)cs * (M - n) + psz * (double)rs * (M - n + 1 + n + 1));
+    r5.log_kind = P_YINV_LEVEL;
+    r5.bytes = fszd * (double)cs * (M - n) + psz * (double)rs * (M - n + 1 + n + 1);
+    out.push_back(r5);
   }
 
   if (zvel_out) {
-    YFwdArgs zf{};
+    PassRec rz;
+    rz.kind = L_YFWD;
+    rz.mode = YF_RHS;
+    rz.gx = ygrid(c, g.yf);
+    rz.gy = 4;
+    YFwdArgs& zf = rz.yf;
     zf.geo = c->geo;
+    zf.ycount = 4;
     zf.lp = g.yf.lp;
     zf.phys = c->phys;
     zf.ex = c->ETAX();
@@ -618,20 +721,32 @@ int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, dou
     zf.which_base = 2;
     zf.vout = zb;
     zf.rows_out = c->h + 1;
-    g.yfwd[YF_RHS]<<<dim3(ygrid(c, g.yf), 4), g.yf.threads, g.yf.smem, c->st>>>(zf, g.twh, g.twy);
-    XFwdArgs xz{};
+    out.push_back(rz);
+    PassRec rx;
+    rx.kind = L_XFWD;
+    rx.mode = XF_PLAIN;
+    rx.gx = xgrid(c, g.xf);
+    rx.gy = 4;
+    XFwdArgs& xz = rx.xf;
     xz.geo = c->geo;
+    xz.ycount = 4;
     xz.rows = c->h + 1;
     xz.vin0 = zb;
     xz.out_spec = zvel_out;
     xz.addk_mask = 1 | (L >= 2 ? 2 : 0);  // W^(1) belongs to W^(M) always and to W^(M-2) when L >= 2
     xz.u_add = uin;
-    g.xfwd[XF_PLAIN]<<<dim3(xgrid(c, g.xf), 4), g.xf.threads, g.xf.smem, c->st>>>(xz, g.twx);
-    return HOS_OK;
+    out.push_back(rx);
+    return;
   }
 
-  YFwdArgs ff{};
+  PassRec r6;
+  r6.kind = L_YFWD;
+  r6.mode = YF_RHS;
+  r6.gx = ygrid(c, g.yf);
+  r6.gy = 2;
+  YFwdArgs& ff = r6.yf;
   ff.geo = c->geo;
+  ff.ycount = 2;
   ff.lp = g.yf.lp;
   ff.phys = c->phys;
   ff.ex = c->ETAX();
@@ -642,11 +757,18 @@ int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, dou
   for (int n = 0; n <= L; n++) ff.w_idx[n] = c->W(n);
   ff.vout = zb;
   ff.rows_out = c->geo.my;
-  g.yfwd[YF_RHS]<<<dim3(ygrid(c, g.yf), 2), g.yf.threads, g.yf.smem, c->st>>>(ff, g.twh, g.twy);
-  log_pass(c, lg, P_YFWD_RHS, psz * (double)rs * (5 + L) + 2.0 * my * nxd * (double)cs);
+  r6.log_kind = P_YFWD_RHS;
+  r6.bytes = psz * (double)rs * (5 + L) + 2.0 * my * nxd * (double)cs;
+  out.push_back(r6);
 
-  XFwdArgs xe{};
+  PassRec r7;
+  r7.kind = L_XFWD;
+  r7.mode = XF_RHS;
+  r7.gx = xgrid(c, g.xf);
+  r7.gy = 2;
+  XFwdArgs& xe = r7.xf;
   xe.geo = c->geo;
+  xe.ycount = 2;
   xe.rows = c->h + 1;
   xe.rows_dev = rows_dev;
   xe.rows_fft = c->geo.my;
@@ -664,13 +786,35 @@ int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, dou
     xe.cfin[p] = dt * c->c[p];
   }
   xe.nstage = c->nst;
-  g.xfwd[XF_RHS]<<<dim3(xgrid(c, g.xf), 2), g.xf.threads, g.xf.smem, c->st>>>(xe, g.twx);
-  {
-    // V rows < my in, stage input (u + earlier k) rows < act, k_s rows < my out;
-    // on the last stage also the other k's and the updated u (rows < my)
-    double b = 2.0 * my * nxd * (double)cs + act * nxd * 16.0 * 2 * (1 + nk) + my * nxd * 16.0 * 2;
-    if (xe.final_update) b += my * nxd * 16.0 * 2 * (c->nst - 1) + my * nxd * 16.0 * 2;
-    log_pass(c, lg, P_XFWD_RHS, b);
+  // V rows < my in, stage input rows < act, k_s rows < my out; on the last
+  // stage also the other k's and the updated u (rows < my)
+  double b = 2.0 * my * nxd * (double)cs + act * nxd * 16.0 * 2 + my * nxd * 16.0 * 2;
+  if (xe.final_update) b += my * nxd * 16.0 * 2 * (c->nst - 1) + my * nxd * 16.0 * 2;
+  r7.log_kind = P_XFWD_RHS;
+  r7.bytes = b;
+  out.push_back(r7);
+}
+
+// Launches one pass of one field with its arguments by value.
+void launch_single(hos_ctx* c, const PassRec& r) {
+  const PassCfg& g = c->cfg;
+  const dim3 grid(r.gx, r.gy);
+  switch (r.kind) {
+    case L_XINV: g.xinv[r.mode]<<<grid, g.xi.threads, g.xi.smem, c->st>>>(r.xi, nullptr, g.twx); break;
+    case L_XFWD: g.xfwd[r.mode]<<<grid, g.xf.threads, g.xf.smem, c->st>>>(r.xf, nullptr, g.twx); break;
+    case L_YINV: g.yinv[r.mode]<<<grid, g.yi.threads, g.yi.smem, c->st>>>(r.yi, nullptr, g.twh, g.twy); break;
+    default: g.yfwd[r.mode]<<<grid, g.yf.threads, g.yf.smem, c->st>>>(r.yf, nullptr, g.twh, g.twy); break;
+  }
+}
+
+// Enqueues one RK stage (see build_stage) on the handle's stream.
+int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, double2* kout, const double* tsrc,
+                  const int* rows_dev, PassLog* lg = nullptr, double2* zvel_out = nullptr) {
+  std::vector<PassRec> recs;
+  build_stage(c, s, dt, rhs_only, uin, kout, tsrc, rows_dev, zvel_out, lg ? lg->act_rows : 0, recs);
+  for (const PassRec& r : recs) {
+    launch_single(c, r);
+    log_pass(c, lg, r.log_kind, r.bytes);
   }
   return HOS_OK;
 }
@@ -718,17 +862,19 @@ int enqueue_r2c(hos_ctx* c, const double* phys_in, double2* spec_out, int dealia
   YFwdArgs fa{};
   fa.geo = c->geo;
   fa.lp = g.yf.lp;
+  fa.ycount = 1;
   fa.in_ptr = phys_in;
   fa.vout = c->zplain;
   fa.rows_out = c->h + 1;
-  g.yfwd[YF_PLAIN]<<<dim3(ygrid(c, g.yf), 1), g.yf.threads, g.yf.smem, c->st>>>(fa, g.twh, g.twy);
+  g.yfwd[YF_PLAIN]<<<dim3(ygrid(c, g.yf), 1), g.yf.threads, g.yf.smem, c->st>>>(fa, nullptr, g.twh, g.twy);
   XFwdArgs xf{};
   xf.geo = c->geo;
   xf.rows = c->h + 1;
+  xf.ycount = 1;
   xf.vin0 = c->zplain;
   xf.out_spec = spec_out;
   xf.dealias = dealias;
-  g.xfwd[XF_PLAIN]<<<dim3(xgrid(c, g.xf), 1), g.xf.threads, g.xf.smem, c->st>>>(xf, g.twx);
+  g.xfwd[XF_PLAIN]<<<dim3(xgrid(c, g.xf), 1), g.xf.threads, g.xf.smem, c->st>>>(xf, nullptr, g.twx);
   return HOS_OK;
 }
 
@@ -737,9 +883,10 @@ int enqueue_c2r(hos_ctx* c, const double2* spec_in, double* phys_out) {
   XInvArgs xa{};
   xa.geo = c->geo;
   xa.rows = c->h + 1;
+  xa.ycount = 1;
   xa.u = spec_in;
   xa.z = c->zplain;
-  g.xinv[XI_PLAIN]<<<dim3(xgrid(c, g.xi), 1), g.xi.threads, g.xi.smem, c->st>>>(xa, g.twx);
+  g.xinv[XI_PLAIN]<<<dim3(xgrid(c, g.xi), 1), g.xi.threads, g.xi.smem, c->st>>>(xa, nullptr, g.twx);
   YInvArgs ya{};
   ya.geo = c->geo;
   ya.lp = g.yi.lp;
@@ -747,7 +894,8 @@ int enqueue_c2r(hos_ctx* c, const double2* spec_in, double* phys_out) {
   ya.rows_in = c->h + 1;
   ya.phys = phys_out;
   ya.jobs[0] = YJob{0, 0, 0};
-  g.yinv[YI_JOBS]<<<dim3(ygrid(c, g.yi), 1), g.yi.threads, g.yi.smem, c->st>>>(ya, g.twh, g.twy);
+  ya.ycount = 1;
+  g.yinv[YI_JOBS]<<<dim3(ygrid(c, g.yi), 1), g.yi.threads, g.yi.smem, c->st>>>(ya, nullptr, g.twh, g.twy);
   return HOS_OK;
 }
 
@@ -781,6 +929,193 @@ int dalloc(P** p, size_t bytes) {
                 cudaGetErrorString(e));
   }
   return HOS_OK;
+}
+
+
+// ---------------------------------------------------------------- ensembles
+// Fields of one size class (same grid, precision, scheme and kernel shapes)
+// advance together: every pass is one launch whose blockIdx.z selects the
+// member, with the member's arguments read from a device array.  Classes run
+// on their own streams, forked from and joined to the ensemble's stream; a
+// whole RK step of all classes is one CUDA graph.
+struct EnsClass {
+  std::vector<int> idx;  // members
+  cudaStream_t st = nullptr;
+  cudaEvent_t join = nullptr;
+};
+
+}  // namespace
+
+struct hos_ens {
+  std::vector<hos_ctx*> mem;
+  std::vector<double> dt;
+  std::vector<EnsClass> cls;
+  cudaStream_t st = nullptr;
+  cudaEvent_t fork = nullptr;
+  void* dargs = nullptr;
+  size_t dargs_bytes = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  int launches_per_step = 0;
+};
+
+namespace {
+
+bool same_class(const hos_ctx* a, const hos_ctx* b) {
+  return a->nx == b->nx && a->ny == b->ny && a->prec == b->prec && a->p.scheme == b->p.scheme &&
+         a->cfg.ec.xi == b->cfg.ec.xi && a->cfg.ec.xf == b->cfg.ec.xf && a->cfg.ec.yi == b->cfg.ec.yi &&
+         a->cfg.ec.yf == b->cfg.ec.yf && a->device == b->device;
+}
+
+// Slot of the r-th pass of a member with L levels in a class whose deepest
+// member has Lmax levels: K1, K2, 3 per level, then the two RHS passes.
+int slot_of(int r, int L, int Lmax, int npass) {
+  if (r < 2 + 3 * L) return r;
+  return 2 + 3 * Lmax + (r - (npass - 2));
+}
+
+struct BatchLaunch {
+  int kind, mode, gx, gy, gz;
+  size_t off;  // byte offset of the argument array in the device buffer
+};
+
+// Builds the launches of one RK step of an ensemble and the host image of
+// their argument arrays.
+void plan_step(hos_ens* E, std::vector<std::vector<BatchLaunch>>& per_class, std::vector<unsigned char>& img,
+               std::vector<StepEndArgs>& ends, std::vector<size_t>& end_off) {
+  per_class.assign(E->cls.size(), {});
+  auto put = [&](const void* p, size_t n) {
+    size_t off = (img.size() + 255) & ~(size_t)255;
+    img.resize(off + n);
+    std::memcpy(img.data() + off, p, n);
+    return off;
+  };
+  for (size_t ci = 0; ci < E->cls.size(); ci++) {
+    const EnsClass& K = E->cls[ci];
+    const int nst = E->mem[K.idx[0]]->nst;
+    int Lmax = 0;
+    for (int f : K.idx) Lmax = std::max(Lmax, E->mem[f]->L);
+    const int nslot = 2 + 3 * Lmax + 2;
+    for (int s = 0; s < nst; s++) {
+      std::vector<std::vector<PassRec>> bys(nslot);
+      for (int f : K.idx) {
+        hos_ctx* c = E->mem[f];
+        std::vector<PassRec> recs;
+        build_stage(c, s, E->dt[f], false, c->u, c->k + (size_t)s * 2 * c->fsz, c->tdev, c->actdev, nullptr, 0, recs);
+        for (size_t r = 0; r < recs.size(); r++) bys[slot_of((int)r, c->L, Lmax, (int)recs.size())].push_back(recs[r]);
+      }
+      for (int sl = 0; sl < nslot; sl++) {
+        const std::vector<PassRec>& v = bys[sl];
+        if (v.empty()) continue;
+        BatchLaunch b;
+        b.kind = v[0].kind;
+        b.mode = v[0].mode;
+        b.gx = v[0].gx;
+        b.gy = 0;
+        b.gz = (int)v.size();
+        for (const PassRec& r : v) b.gy = std::max(b.gy, r.gy);
+        if (b.kind == L_XINV) {
+          std::vector<XInvArgs> a;
+          for (const PassRec& r : v) a.push_back(r.xi);
+          b.off = put(a.data(), a.size() * sizeof(XInvArgs));
+        } else if (b.kind == L_XFWD) {
+          std::vector<XFwdArgs> a;
+          for (const PassRec& r : v) a.push_back(r.xf);
+          b.off = put(a.data(), a.size() * sizeof(XFwdArgs));
+        } else if (b.kind == L_YINV) {
+          std::vector<YInvArgs> a;
+          for (const PassRec& r : v) a.push_back(r.yi);
+          b.off = put(a.data(), a.size() * sizeof(YInvArgs));
+        } else {
+          std::vector<YFwdArgs> a;
+          for (const PassRec& r : v) a.push_back(r.yf);
+          b.off = put(a.data(), a.size() * sizeof(YFwdArgs));
+        }
+        per_class[ci].push_back(b);
+      }
+    }
+    std::vector<StepEndArgs> se;
+    for (int f : K.idx) {
+      hos_ctx* c = E->mem[f];
+      se.push_back(StepEndArgs{c->ham_part, xgrid(c, c->cfg.xf), c->tdev, E->dt[f], c->stepdev, c->ham_hist,
+                               c->t_hist, HIST_CAP});
+    }
+    end_off.push_back(put(se.data(), se.size() * sizeof(StepEndArgs)));
+    ends.insert(ends.end(), se.begin(), se.end());
+  }
+}
+
+int build_ens_graph(hos_ens* E) {
+  std::vector<std::vector<BatchLaunch>> per_class;
+  std::vector<unsigned char> img;
+  std::vector<StepEndArgs> ends;
+  std::vector<size_t> end_off;
+  plan_step(E, per_class, img, ends, end_off);
+  if (img.size() > E->dargs_bytes) {
+    if (E->dargs) cudaFree(E->dargs);
+    E->dargs = nullptr;
+    E->dargs_bytes = 0;
+    int rc = dalloc(&E->dargs, img.size());
+    if (rc) return rc;
+    E->dargs_bytes = img.size();
+  }
+  HOS_CK(cudaMemcpy(E->dargs, img.data(), img.size(), cudaMemcpyHostToDevice));
+  if (E->gexec) cudaGraphExecDestroy(E->gexec);
+  if (E->graph) cudaGraphDestroy(E->graph);
+  E->gexec = nullptr;
+  E->graph = nullptr;
+  E->launches_per_step = 0;
+  HOS_CK(cudaStreamBeginCapture(E->st, cudaStreamCaptureModeThreadLocal));
+  cudaEventRecord(E->fork, E->st);
+  char* base = reinterpret_cast<char*>(E->dargs);
+  for (size_t ci = 0; ci < E->cls.size(); ci++) {
+    const EnsClass& K = E->cls[ci];
+    const PassCfg& g = E->mem[K.idx[0]]->cfg;
+    cudaStreamWaitEvent(K.st, E->fork, 0);
+    for (const BatchLaunch& b : per_class[ci]) {
+      const dim3 grid(b.gx, b.gy, b.gz);
+      void* a = base + b.off;
+      switch (b.kind) {
+        case L_XINV:
+          g.xinv_b[b.mode]<<<grid, g.xi.threads, g.xi.smem, K.st>>>(XInvArgs{}, (const XInvArgs*)a, g.twx);
+          break;
+        case L_XFWD:
+          g.xfwd_b[b.mode]<<<grid, g.xf.threads, g.xf.smem, K.st>>>(XFwdArgs{}, (const XFwdArgs*)a, g.twx);
+          break;
+        case L_YINV:
+          g.yinv_b[b.mode]<<<grid, g.yi.threads, g.yi.smem, K.st>>>(YInvArgs{}, (const YInvArgs*)a, g.twh, g.twy);
+          break;
+        default:
+          g.yfwd_b[b.mode]<<<grid, g.yf.threads, g.yf.smem, K.st>>>(YFwdArgs{}, (const YFwdArgs*)a, g.twh, g.twy);
+          break;
+      }
+      E->launches_per_step++;
+    }
+    k_step_end_b<<<(unsigned)K.idx.size(), 256, 0, K.st>>>((const StepEndArgs*)(base + end_off[ci]));
+    E->launches_per_step++;
+    cudaEventRecord(K.join, K.st);
+    cudaStreamWaitEvent(E->st, K.join, 0);
+  }
+  cudaGraph_t gr = nullptr;
+  cudaError_t err = cudaStreamEndCapture(E->st, &gr);
+  HOS_CK(err);
+  E->graph = gr;
+  HOS_CK(cudaGraphInstantiate(&E->gexec, E->graph, 0));
+  return HOS_OK;
+}
+
+void release_ens(hos_ens* E) {
+  if (!E) return;
+  if (E->gexec) cudaGraphExecDestroy(E->gexec);
+  if (E->graph) cudaGraphDestroy(E->graph);
+  if (E->dargs) cudaFree(E->dargs);
+  for (EnsClass& K : E->cls) {
+    if (K.join) cudaEventDestroy(K.join);
+    if (K.st) cudaStreamDestroy(K.st);
+  }
+  if (E->fork) cudaEventDestroy(E->fork);
+  if (E->st) cudaStreamDestroy(E->st);
+  delete E;
 }
 
 }  // namespace
@@ -1238,6 +1573,88 @@ int hos_hamiltonian(hos_handle h, const double* eta, const double* eta_t, const 
   HOS_CK(cudaMemcpyAsync(&r, h->hpart + h->h + 1, sizeof(double), cudaMemcpyDeviceToHost, h->st));
   HOS_CK(cudaStreamSynchronize(h->st));
   *H = r;
+  return HOS_OK;
+}
+
+int hos_ensemble_create(const hos_handle* members, const double* dt, int n, hos_ensemble* out) {
+  if (!members || !dt || !out || n < 1) return fail(HOS_ERR_ARG, "bad argument");
+  *out = nullptr;
+  hos_ens* E = new hos_ens();
+  for (int i = 0; i < n; i++) {
+    if (!members[i]) {
+      delete E;
+      return fail(HOS_ERR_ARG, "null member %d", i);
+    }
+    for (int j = 0; j < i; j++)
+      if (members[j] == members[i]) {
+        delete E;
+        return fail(HOS_ERR_ARG, "member %d appears twice", i);
+      }
+    E->mem.push_back(members[i]);
+    E->dt.push_back(dt[i]);
+  }
+  for (int i = 0; i < n; i++) {
+    size_t ci = 0;
+    for (; ci < E->cls.size(); ci++)
+      if (same_class(E->mem[E->cls[ci].idx[0]], E->mem[i])) break;
+    if (ci == E->cls.size()) E->cls.emplace_back();
+    if (E->cls[ci].idx.size() >= 65535) {
+      release_ens(E);
+      return fail(HOS_ERR_ARG, "more than 65535 members of one size class");
+    }
+    E->cls[ci].idx.push_back(i);
+  }
+  cudaError_t err = cudaStreamCreateWithFlags(&E->st, cudaStreamNonBlocking);
+  if (err == cudaSuccess) err = cudaEventCreateWithFlags(&E->fork, cudaEventDisableTiming);
+  for (EnsClass& K : E->cls) {
+    if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&K.st, cudaStreamNonBlocking);
+    if (err == cudaSuccess) err = cudaEventCreateWithFlags(&K.join, cudaEventDisableTiming);
+  }
+  if (err != cudaSuccess) {
+    release_ens(E);
+    return fail(HOS_ERR_CUDA, "ensemble streams: %s", cudaGetErrorString(err));
+  }
+  // members' pending work (state uploads) completes before the first step
+  for (hos_ctx* c : E->mem) {
+    err = cudaStreamSynchronize(c->st);
+    if (err != cudaSuccess) {
+      release_ens(E);
+      return fail(HOS_ERR_CUDA, "member sync: %s", cudaGetErrorString(err));
+    }
+  }
+  int rc = build_ens_graph(E);
+  if (rc) {
+    release_ens(E);
+    return rc;
+  }
+  *out = E;
+  return HOS_OK;
+}
+
+int hos_ensemble_step(hos_ensemble e, int nsteps) {
+  if (!e || nsteps < 0) return fail(HOS_ERR_ARG, "bad argument");
+  for (int i = 0; i < nsteps; i++) HOS_CK(cudaGraphLaunch(e->gexec, e->st));
+  return HOS_OK;
+}
+
+int hos_ensemble_sync(hos_ensemble e) {
+  if (!e) return fail(HOS_ERR_ARG, "null ensemble");
+  HOS_CK(cudaStreamSynchronize(e->st));
+  HOS_CK(cudaGetLastError());
+  return HOS_OK;
+}
+
+int hos_ensemble_info(hos_ensemble e, int* nclasses, int* launches_per_step) {
+  if (!e) return fail(HOS_ERR_ARG, "null ensemble");
+  if (nclasses) *nclasses = (int)e->cls.size();
+  if (launches_per_step) *launches_per_step = e->launches_per_step;
+  return HOS_OK;
+}
+
+int hos_ensemble_destroy(hos_ensemble e) {
+  if (!e) return HOS_OK;
+  cudaStreamSynchronize(e->st);
+  release_ens(e);
   return HOS_OK;
 }
 

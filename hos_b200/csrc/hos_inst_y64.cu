@@ -3,14 +3,14 @@
 
 namespace hos {
 
-template <int H, int E, int M>
+template <int H, int E, int M, bool BT>
 constexpr YInvFn yinv_fn() {
-  if constexpr (elems_valid(0, H, E)) return &k_yinv<double, H, E, M>;
+  if constexpr (elems_valid(0, H, E)) return &k_yinv<double, H, E, M, BT>;
   else return nullptr;
 }
-template <int H, int E, int M>
+template <int H, int E, int M, bool BT>
 constexpr YFwdFn yfwd_fn() {
-  if constexpr (elems_valid(0, H, E)) return &k_yfwd<double, H, E, M>;
+  if constexpr (elems_valid(0, H, E)) return &k_yfwd<double, H, E, M, BT>;
   else return nullptr;
 }
 
@@ -19,56 +19,56 @@ constexpr YFwdFn yfwd_fn() {
 
 #define HOS_CASE_I(H, E, M) \
   case H:                   \
-    return yinv_fn<H, E, M>();
+    return yinv_fn<H, E, M, BT>();
 #define HOS_CASE_F(H, E, M) \
   case H:                   \
-    return yfwd_fn<H, E, M>();
+    return yfwd_fn<H, E, M, BT>();
 
-template <int E, int M>
+template <int E, int M, bool BT>
 static YInvFn yinv_n(int h) {
   switch (h) {
     HOS_SIZES(HOS_CASE_I, E, M)
     default: return nullptr;
   }
 }
-template <int E, int M>
+template <int E, int M, bool BT>
 static YFwdFn yfwd_n(int h) {
   switch (h) {
     HOS_SIZES(HOS_CASE_F, E, M)
     default: return nullptr;
   }
 }
-template <int M>
+template <int M, bool BT>
 static YInvFn yinv_e(int h, int e) {
   switch (e) {
-    case 8: return yinv_n<8, M>(h);
-    case 16: return yinv_n<16, M>(h);
-    case 32: return yinv_n<32, M>(h);
+    case 8: return yinv_n<8, M, BT>(h);
+    case 16: return yinv_n<16, M, BT>(h);
+    case 32: return yinv_n<32, M, BT>(h);
     default: return nullptr;
   }
 }
-template <int M>
+template <int M, bool BT>
 static YFwdFn yfwd_e(int h, int e) {
   switch (e) {
-    case 8: return yfwd_n<8, M>(h);
-    case 16: return yfwd_n<16, M>(h);
-    case 32: return yfwd_n<32, M>(h);
+    case 8: return yfwd_n<8, M, BT>(h);
+    case 16: return yfwd_n<16, M, BT>(h);
+    case 32: return yfwd_n<32, M, BT>(h);
     default: return nullptr;
   }
 }
 
-YInvFn lookup_yinv_64(int mode, int h, int e) {
+YInvFn lookup_yinv_64(int mode, int h, int e, bool batch) {
   switch (mode) {
-    case YI_JOBS: return yinv_e<YI_JOBS>(h, e);
-    case YI_LEVEL: return yinv_e<YI_LEVEL>(h, e);
+    case YI_JOBS: return batch ? yinv_e<YI_JOBS, true>(h, e) : yinv_e<YI_JOBS, false>(h, e);
+    case YI_LEVEL: return batch ? yinv_e<YI_LEVEL, true>(h, e) : yinv_e<YI_LEVEL, false>(h, e);
     default: return nullptr;
   }
 }
-YFwdFn lookup_yfwd_64(int mode, int h, int e) {
+YFwdFn lookup_yfwd_64(int mode, int h, int e, bool batch) {
   switch (mode) {
-    case YF_PLAIN: return yfwd_e<YF_PLAIN>(h, e);
-    case YF_LEVEL: return yfwd_e<YF_LEVEL>(h, e);
-    case YF_RHS: return yfwd_e<YF_RHS>(h, e);
+    case YF_PLAIN: return batch ? nullptr : yfwd_e<YF_PLAIN, false>(h, e);
+    case YF_LEVEL: return batch ? yfwd_e<YF_LEVEL, true>(h, e) : yfwd_e<YF_LEVEL, false>(h, e);
+    case YF_RHS: return batch ? yfwd_e<YF_RHS, true>(h, e) : yfwd_e<YF_RHS, false>(h, e);
     default: return nullptr;
   }
 }

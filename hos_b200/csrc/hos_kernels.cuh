@@ -70,6 +70,7 @@ enum { YF_PLAIN = 0, YF_LEVEL = 1, YF_RHS = 2 };
 // ---------------------------------------------------------------- x inverse
 struct XInvArgs {
   Geo geo;
+  int ycount;           // batched launches: blocks with blockIdx.y >= ycount have no work
   int rows;             // ky rows that may be nonzero in the input
   const int* rows_dev;  // if set, overrides rows (active rows of the state, kept on the device)
   const double2* u;     // STAGE: packed state [2][h+1][nx]; PLAIN: one field
@@ -88,8 +89,11 @@ struct XInvArgs {
 // STAGE outputs (blockIdx.y = o): 0 eta, 1 i kx eta, 2 phi, 3 i kx phi,
 // 3+p d_z^p phi (p >= 1).  The stage input u + sum coef*k is formed on the
 // fly (time_schemes_par.c:38-67).
-template <typename T, int NX, int E, int MODE>
-__global__ void __launch_bounds__(MAX_THREADS, 2) k_xinv(const __grid_constant__ XInvArgs a, const void* twv) {
+template <typename T, int NX, int E, int MODE, bool B>
+__global__ void __launch_bounds__(MAX_THREADS, 2) k_xinv(const __grid_constant__ XInvArgs a0,
+                                                         const XInvArgs* __restrict__ arr, const void* twv) {
+  const XInvArgs& a = B ? arr[blockIdx.z] : a0;  // batched: one field per z
+  if (B && (int)blockIdx.y >= a.ycount) return;
   using C = cpx<T>;
   constexpr int P = NX / E;
   const C* tw = reinterpret_cast<const C*>(twv);
@@ -159,6 +163,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_xinv(const __grid_constant__
 // ---------------------------------------------------------------- x forward
 struct XFwdArgs {
   Geo geo;
+  int ycount;           // batched launches: blocks with blockIdx.y >= ycount have no work
   int rows;             // rows processed
   const int* rows_dev;  // if set, overrides rows
   int rows_fft;         // RHS: rows < rows_fft are transformed; rows in [rows_fft, rows) only add to the Hamiltonian
@@ -184,8 +189,11 @@ struct XFwdArgs {
   int nstage;                     // number of stages; k of the last one is in registers
 };
 
-template <typename T, int NX, int E, int MODE>
-__global__ void __launch_bounds__(MAX_THREADS, 2) k_xfwd(const __grid_constant__ XFwdArgs a, const void* twv) {
+template <typename T, int NX, int E, int MODE, bool B>
+__global__ void __launch_bounds__(MAX_THREADS, 2) k_xfwd(const __grid_constant__ XFwdArgs a0,
+                                                         const XFwdArgs* __restrict__ arr, const void* twv) {
+  const XFwdArgs& a = B ? arr[blockIdx.z] : a0;
+  if (B && (int)blockIdx.y >= a.ycount) return;
   using C = cpx<T>;
   constexpr int P = NX / E;
   const C* tw = reinterpret_cast<const C*>(twv);
@@ -339,6 +347,7 @@ struct YJob {
 
 struct YInvArgs {
   Geo geo;
+  int ycount;           // batched launches: blocks with blockIdx.y >= ycount have no work
   int lp;            // line pitch in shared memory (complex elements)
   const void* z;     // Z arrays (T2), stride (h+1)*nx
   int rows_in;       // Z rows that may be nonzero; the rest are read as zero
@@ -354,9 +363,12 @@ struct YInvArgs {
   int w_in[MAX_TERMS];
 };
 
-template <typename T, int H, int E, int MODE>
-__global__ void __launch_bounds__(MAX_THREADS, 2) k_yinv(const __grid_constant__ YInvArgs a, const void* twv,
+template <typename T, int H, int E, int MODE, bool B>
+__global__ void __launch_bounds__(MAX_THREADS, 2) k_yinv(const __grid_constant__ YInvArgs a0,
+                                                         const YInvArgs* __restrict__ arr, const void* twv,
                                                          const void* twyv) {
+  const YInvArgs& a = B ? arr[blockIdx.z] : a0;
+  if (B && (int)blockIdx.y >= a.ycount) return;
   using C = cpx<T>;
   constexpr int P = H / E;
   const C* tw = reinterpret_cast<const C*>(twv);    // length H
@@ -394,17 +406,17 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yinv(const __grid_constant__
   for (int e = 0; e < E; e++) {
     const int k = t + e * P;
     C A = tl[(k)];
-    C B = tl[(H - k)];
+    C Bv = tl[(H - k)];
     if (J.iky) {
       const T ka = (T)ky_of(geo, k), kb = (T)ky_of(geo, H - k);
       A = cscale(cmul_i(A), ka);
-      B = cscale(cmul_i(B), kb);
+      Bv = cscale(cmul_i(Bv), kb);
     }
     if (k == 0) {  // FFTW c2r ignores Im of the ky = 0 and ky = Ny/2 bins
       A.y = (T)0;
-      B.y = (T)0;
+      Bv.y = (T)0;
     }
-    const C Bc = cconj(B);
+    const C Bc = cconj(Bv);
     const C xe = cadd(A, Bc);
     const C d = csub(A, Bc);
     const C w = cconj(__ldg(&twy[k]));  // exp(+2 pi i k / Ny)
@@ -444,6 +456,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yinv(const __grid_constant__
 
 struct YFwdArgs {
   Geo geo;
+  int ycount;           // batched launches: blocks with blockIdx.y >= ycount have no work
   int lp;
   const void* phys;   // physical arrays (T), stride nx*ny
   const void* in_ptr; // PLAIN: physical input (T) [nx][ny]
@@ -501,9 +514,12 @@ __device__ __forceinline__ T rhs_point(const YFwdArgs& a, const T* W, T ex, T ey
   return (T)0.5 * (w2m + grad2 * w2m2) - (T)0.5 * (px * px + py * py);  // hosm_2d_par.c:181-206
 }
 
-template <typename T, int H, int E, int MODE>
-__global__ void __launch_bounds__(MAX_THREADS, 2) k_yfwd(const __grid_constant__ YFwdArgs a, const void* twv,
+template <typename T, int H, int E, int MODE, bool B>
+__global__ void __launch_bounds__(MAX_THREADS, 2) k_yfwd(const __grid_constant__ YFwdArgs a0,
+                                                         const YFwdArgs* __restrict__ arr, const void* twv,
                                                          const void* twyv) {
+  const YFwdArgs& a = B ? arr[blockIdx.z] : a0;
+  if (B && (int)blockIdx.y >= a.ycount) return;
   using C = cpx<T>;
   constexpr int P = H / E;
   const C* tw = reinterpret_cast<const C*>(twv);

@@ -140,7 +140,7 @@ extern "C" int hos_fft_2d_noalloc(const double* u_phys, double* hu, int nx, int 
   fa.in_ptr = u_phys;
   fa.vout = d->spec;
   fa.rows_out = h + 1;
-  yf<<<dim3(nx / gy, 1), gy * py, (size_t)gy * lp * sizeof(double2), st>>>(fa, d->tw + NOALLOC_MAX_LEN,
+  yf<<<dim3(nx / gy, 1), gy * py, (size_t)gy * lp * sizeof(double2), st>>>(fa, nullptr, d->tw + NOALLOC_MAX_LEN,
                                                                             d->tw + 2 * NOALLOC_MAX_LEN);
   XFwdArgs xa{};
   xa.geo = geo;
@@ -148,7 +148,7 @@ extern "C" int hos_fft_2d_noalloc(const double* u_phys, double* hu, int nx, int 
   xa.vin0 = d->spec;
   xa.out_spec = reinterpret_cast<double2*>(hu);
   xa.dealias = 0;
-  xf<<<dim3((h + 1 + gx - 1) / gx, 1), gx * px, (size_t)gx * nx * sizeof(double2), st>>>(xa, d->tw);
+  xf<<<dim3((h + 1 + gx - 1) / gx, 1), gx * px, (size_t)gx * nx * sizeof(double2), st>>>(xa, nullptr, d->tw);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(HOS_ERR_CUDA, cudaGetErrorString(e));
   return HOS_OK;

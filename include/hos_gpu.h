@@ -152,6 +152,22 @@ typedef struct hos_pass_stat {
 } hos_pass_stat;
 int hos_profile_stage(hos_handle h, double dt, int reps, hos_pass_stat* out, int max, int* count);
 
+/* Ensembles (many independent fields advanced together).  Members are
+ * existing handles of any grid, order, precision and dt; members with the
+ * same grid, precision and scheme form a size class whose every pass is one
+ * launch over all its members (blockIdx.z = member), and one RK step of all
+ * classes is one CUDA graph with the classes on parallel streams.  Each
+ * member advances exactly as hos_step(member, dt[i], 1) would, and keeps
+ * its own state, time and energy record.  No counterpart in the reference
+ * (it advances one field per process). Members must not be stepped on their
+ * own while the ensemble exists; call hos_ensemble_sync before reading them. */
+typedef struct hos_ens* hos_ensemble;
+int hos_ensemble_create(const hos_handle* members, const double* dt, int n, hos_ensemble* out);
+int hos_ensemble_step(hos_ensemble e, int nsteps);
+int hos_ensemble_sync(hos_ensemble e);
+int hos_ensemble_info(hos_ensemble e, int* nclasses, int* launches_per_step);
+int hos_ensemble_destroy(hos_ensemble e);
+
 /* Kernel launches of this library in one RK step of the handle. */
 int hos_launches_per_step(hos_handle h);
 
