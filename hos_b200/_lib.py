@@ -44,6 +44,7 @@ class HosParams(ctypes.Structure):
         ("scheme", ctypes.c_int),
         ("mx", ctypes.c_int),
         ("my", ctypes.c_int),
+        ("tune", ctypes.c_int * 8),
     ]
 
 

@@ -236,7 +236,8 @@ namespace {
 // Elements per thread of each pass kind (x-inverse, x-forward, y-inverse,
 // y-forward); defaults, overridable per handle by the autotuner.
 struct ElemChoice {
-  int xi = 8, xf = 8, yi = 8, yf = 8;
+  int xi = 8, xf = 8, yi = 8, yf = 8;          // elements per thread
+  int sxi = 0, sxf = 0, syi = 0, syf = 0;      // lines per block scaled by 2^s
 };
 
 // Launch geometry of one pass kind: elements per thread E, lines per block,
@@ -417,10 +418,19 @@ struct hos_ctx {
 
 namespace {
 
-int x_geometry(int n, int e, size_t cs, KindCfg* k) {
+int scaled_lines(int base, int scale, int maxl) {
+  int l = base;
+  if (scale > 0) l <<= scale;
+  if (scale < 0) l >>= -scale;
+  if (l > maxl) l = maxl;
+  if (l < 1) l = 1;
+  return l;
+}
+
+int x_geometry(int n, int e, size_t cs, int scale, KindCfg* k) {
   const int P = n / e;
-  int lines = 128 / P;
-  if (lines < 1) lines = 1;
+  int lines = scaled_lines(128 / P > 0 ? 128 / P : 1, scale, MAX_THREADS / P > 0 ? MAX_THREADS / P : 1);
+  if (lines * P < 32) lines = 32 / P;
   k->e = e;
   k->lines = lines;
   k->threads = lines * P;
@@ -429,11 +439,10 @@ int x_geometry(int n, int e, size_t cs, KindCfg* k) {
   return 0;
 }
 
-int y_geometry(int h, int nx, int e, size_t cs, KindCfg* k) {
+int y_geometry(int h, int nx, int e, size_t cs, int scale, KindCfg* k) {
   const int P = h / e;
-  int lines = MAX_THREADS / P;
+  int lines = scaled_lines(MAX_THREADS / P > 0 ? MAX_THREADS / P : 1, scale, MAX_THREADS / P > 0 ? MAX_THREADS / P : 1);
   if (lines > nx) lines = nx;
-  if (lines < 1) lines = 1;
   k->e = e;
   k->lines = lines;
   k->threads = lines * P;
@@ -445,6 +454,8 @@ int y_geometry(int h, int nx, int e, size_t cs, KindCfg* k) {
   k->smem = (size_t)lines * lp * cs;
   return k->threads > MAX_THREADS ? -1 : 0;
 }
+
+std::mutex g_attr_mu;  // serialises the kernel attribute updates of concurrent hos_create calls
 
 // Largest supported E not above `want` for a line of length n.
 int pick_elems(int prec, int n, int want) {
@@ -486,24 +497,31 @@ int make_cfg(hos_ctx* c, int prec, const ElemChoice& ec, PassCfg* o) {
   for (int m = 0; m < 2; m++) o->yinv_b[m] = lookup_yinv(prec, m, c->h, eyi, true);
   for (int m = 0; m < 3; m++) o->yfwd_b[m] = lookup_yfwd(prec, m, c->h, eyf, true);
   o->ec = ec;
-  if (x_geometry(c->nx, exi, cs, &o->xi) || x_geometry(c->nx, exf, cs, &o->xf) ||
-      y_geometry(c->h, c->nx, eyi, cs, &o->yi) || y_geometry(c->h, c->nx, eyf, cs, &o->yf))
+  if (x_geometry(c->nx, exi, cs, ec.sxi, &o->xi) || x_geometry(c->nx, exf, cs, ec.sxf, &o->xf) ||
+      y_geometry(c->h, c->nx, eyi, cs, ec.syi, &o->yi) || y_geometry(c->h, c->nx, eyf, cs, ec.syf, &o->yf))
     return fail(HOS_ERR_ARG, "no launch geometry for %dx%d", c->nx, c->ny);
-  for (int m = 0; m < 2; m++)
-    HOS_CK(cudaFuncSetAttribute((const void*)o->xinv[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->xi.smem));
-  for (int m = 0; m < 3; m++)
-    HOS_CK(cudaFuncSetAttribute((const void*)o->xfwd[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->xf.smem));
-  for (int m = 0; m < 2; m++)
-    HOS_CK(cudaFuncSetAttribute((const void*)o->yinv[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->yi.smem));
-  for (int m = 0; m < 3; m++)
-    HOS_CK(cudaFuncSetAttribute((const void*)o->yfwd[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->yf.smem));
-  auto setb = [](const void* f, size_t smem) -> cudaError_t {
-    return f ? cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) : cudaSuccess;
+  // The dynamic shared memory limit of a kernel is only ever raised: handles
+  // with different shapes (and a handle's compute and boundary passes) share
+  // kernel functions, and lowering the limit would break the larger launch.
+  auto raise = [](const void* f, size_t smem) -> cudaError_t {
+    if (!f) return cudaSuccess;
+    cudaFuncAttributes at;
+    cudaError_t err = cudaFuncGetAttributes(&at, f);
+    if (err != cudaSuccess) return err;
+    if ((size_t)at.maxDynamicSharedSizeBytes >= smem) return cudaSuccess;
+    return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   };
-  for (int m = 0; m < 2; m++) HOS_CK(setb((const void*)o->xinv_b[m], o->xi.smem));
-  for (int m = 0; m < 3; m++) HOS_CK(setb((const void*)o->xfwd_b[m], o->xf.smem));
-  for (int m = 0; m < 2; m++) HOS_CK(setb((const void*)o->yinv_b[m], o->yi.smem));
-  for (int m = 0; m < 3; m++) HOS_CK(setb((const void*)o->yfwd_b[m], o->yf.smem));
+  {
+    std::lock_guard<std::mutex> lk(g_attr_mu);
+    for (int m = 0; m < 2; m++) HOS_CK(raise((const void*)o->xinv[m], o->xi.smem));
+    for (int m = 0; m < 3; m++) HOS_CK(raise((const void*)o->xfwd[m], o->xf.smem));
+    for (int m = 0; m < 2; m++) HOS_CK(raise((const void*)o->yinv[m], o->yi.smem));
+    for (int m = 0; m < 3; m++) HOS_CK(raise((const void*)o->yfwd[m], o->yf.smem));
+    for (int m = 0; m < 2; m++) HOS_CK(raise((const void*)o->xinv_b[m], o->xi.smem));
+    for (int m = 0; m < 3; m++) HOS_CK(raise((const void*)o->xfwd_b[m], o->xf.smem));
+    for (int m = 0; m < 2; m++) HOS_CK(raise((const void*)o->yinv_b[m], o->yi.smem));
+    for (int m = 0; m < 3; m++) HOS_CK(raise((const void*)o->yfwd_b[m], o->yf.smem));
+  }
   o->twx = c->tw[prec][0];
   o->twh = c->tw[prec][1];
   o->twy = c->tw[prec][2];
@@ -964,7 +982,8 @@ namespace {
 bool same_class(const hos_ctx* a, const hos_ctx* b) {
   return a->nx == b->nx && a->ny == b->ny && a->prec == b->prec && a->p.scheme == b->p.scheme &&
          a->cfg.ec.xi == b->cfg.ec.xi && a->cfg.ec.xf == b->cfg.ec.xf && a->cfg.ec.yi == b->cfg.ec.yi &&
-         a->cfg.ec.yf == b->cfg.ec.yf && a->device == b->device;
+         a->cfg.ec.yf == b->cfg.ec.yf && a->cfg.ec.sxi == b->cfg.ec.sxi && a->cfg.ec.sxf == b->cfg.ec.sxf &&
+         a->cfg.ec.syi == b->cfg.ec.syi && a->cfg.ec.syf == b->cfg.ec.syf && a->device == b->device;
 }
 
 // Slot of the r-th pass of a member with L levels in a class whose deepest
@@ -1238,6 +1257,17 @@ int hos_create(const hos_params* p, hos_handle* out) {
   {
     ElemChoice ec = default_elems(c->prec);
     ElemChoice ec64 = default_elems(0);
+    // shapes chosen by the autotuner (hos_params.tune): E per pass kind, then
+    // the lines-per-block scale exponents
+    if (p->tune[0]) ec.xi = p->tune[0];
+    if (p->tune[1]) ec.xf = p->tune[1];
+    if (p->tune[2]) ec.yi = p->tune[2];
+    if (p->tune[3]) ec.yf = p->tune[3];
+    auto clamp3 = [](int v) { return v < -3 ? -3 : (v > 3 ? 3 : v); };
+    ec.sxi = clamp3(p->tune[4]);
+    ec.sxf = clamp3(p->tune[5]);
+    ec.syi = clamp3(p->tune[6]);
+    ec.syf = clamp3(p->tune[7]);
     rc = make_cfg(c, c->prec, ec, &c->cfg);
     if (!rc) rc = make_cfg(c, 0, ec64, &c->cfg64);
   }

@@ -54,6 +54,7 @@ class HosField:
         scheme="rk4",
         mx=None,
         my=None,
+        tune=None,
     ):
         self._lib = _lib.load()
         p = _lib.HosParams()
@@ -67,6 +68,14 @@ class HosField:
         p.scheme = _SCHEMES[scheme] if isinstance(scheme, str) else int(scheme)
         p.mx = int(mx or 0)
         p.my = int(my or 0)
+        if isinstance(tune, str) and tune == "auto":
+            from .autotune import tune as _autotune
+
+            tune = _autotune(int(nx), int(ny), int(order), precision if isinstance(precision, str) else
+                             ("fp32" if int(precision) else "fp64"))
+        if tune is not None:
+            for i, v in enumerate(list(tune)[:8]):
+                p.tune[i] = int(v)
         self.params = p
         self.nx, self.ny, self.h = int(nx), int(ny), int(ny) // 2
         h = ctypes.c_void_p()

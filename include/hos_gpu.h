@@ -63,6 +63,9 @@ typedef struct hos_params {
   double tramp;     /* ramp time scale Tramp */
   int scheme;       /* HOS_RK4 etc. */
   int mx, my;       /* dealias bounds; 0 selects the reference rule (operators_par.c:290-291) */
+  int tune[8];      /* kernel shapes (0 = default): elements per thread of the x-inverse, x-forward,
+                       y-inverse and y-forward passes (8, 16, or 32 in FP32), then the base-2 exponents
+                       scaling their lines per block; chosen by hos_b200.autotune */
 } hos_params;
 
 typedef struct hos_ctx* hos_handle;
