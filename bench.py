@@ -57,6 +57,12 @@ def parse():
     ap.add_argument("--accuracy-steps", type=int, default=1000)
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--ensemble-fields", type=int, default=256)
+    ap.add_argument("--ensemble-steps", type=int, default=500)
+    ap.add_argument("--serve-rate", type=float, default=1.2)
+    ap.add_argument("--serve-duration", type=float, default=20.0)
+    ap.add_argument("--serve-limit", type=float, default=90.0)
     return ap.parse_args()
 
 
@@ -187,6 +193,114 @@ def cpu_reference_rate(args, eta, phi, info, dt, max_seconds):
     return {"value": nsteps / el, "steps": nsteps, "seconds": el}
 
 
+# ------------------------------------------------------------------ ensemble and serving
+def run_ensemble(args, seed=0):
+    """256 independent JONSWAP fields (grids 128/256/512 with weights
+    0.5/0.3/0.2, M in {3,4,5}, kp*Hs/2 uniform in [0.05, 0.12], kp = n/16,
+    half deep water and half finite depth with kp*h uniform in [1, 3]) in
+    FP32 compute / FP64 state, 500 RK4 steps each (dt = Tp/50), advanced as
+    one ensemble; compared with the same fields advanced one after another
+    in plain FP64."""
+    import numpy as np
+    import torch
+
+    from hos_b200 import HosEnsemble, HosField
+    from hos_b200.serve import _dptr, jonswap_device
+
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(args.ensemble_fields):
+        n = int(rng.choice([128, 256, 512], p=[0.5, 0.3, 0.2]))
+        M = int(rng.choice([3, 4, 5]))
+        kp = n / 16.0
+        depth = None if i % 2 == 0 else float(rng.uniform(1.0, 3.0)) / kp
+        specs.append((n, M, kp, float(rng.uniform(0.05, 0.12)), depth, 7000 + i))
+    fields, dts, hs = [], [], []
+    for (n, M, kp, st, depth, sd) in specs:
+        eta, phi, tp = jonswap_device(n, kp, st, sd, depth=depth)
+        f = HosField(n, n, order=M, precision="fp32", depth=depth, tune="auto")
+        f._lib.hos_set_state_physical(f._h, _dptr(eta), _dptr(phi), 0.0)
+        fields.append(f)
+        dts.append(tp / 50)
+        hs.append(2 * st / kp)
+    ens = HosEnsemble(fields, dts)
+    ens.step(3)
+    ens.sync()
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(ens._lib.hos_stream(fields[0]._h))
+    t0 = time.perf_counter()
+    ens.step(args.ensemble_steps)
+    ens.sync()
+    el = time.perf_counter() - t0
+    gp = sum(n * n for (n, *_r) in specs) * args.ensemble_steps
+    info = ens.info
+    ens.close()
+    # sequential plain FP64: each (n, M, depth?) kind timed alone, weighted by the mix
+    seq_s = 0.0
+    rates = {}
+    for (n, M, kp, st, depth, sd) in specs:
+        key = (n, M, depth is not None)
+        if key not in rates:
+            eta, phi, tp = jonswap_device(n, kp, st, sd, depth=depth)
+            g = HosField(n, n, order=M, precision="fp64", depth=depth)
+            g._lib.hos_set_state_physical(g._h, _dptr(eta), _dptr(phi), 0.0)
+            g.step(tp / 50, 3)
+            g.sync()
+            t1 = time.perf_counter()
+            g.step(tp / 50, 30)
+            g.sync()
+            rates[key] = (time.perf_counter() - t1) / 30
+            g.close()
+        seq_s += rates[key] * args.ensemble_steps
+    # accuracy of the FP32 members: four members rerun in FP64
+    errs = []
+    for i in range(4):
+        (n, M, kp, st, depth, sd) = specs[i]
+        eta, phi, tp = jonswap_device(n, kp, st, sd, depth=depth)
+        g = HosField(n, n, order=M, precision="fp64", depth=depth)
+        g._lib.hos_set_state_physical(g._h, _dptr(eta), _dptr(phi), 0.0)
+        g.step(tp / 50, args.ensemble_steps + 3)
+        e64, _ = g.state_physical()
+        e32, _ = fields[i].state_physical()
+        errs.append(float(np.max(np.abs(e32 - e64)) / hs[i]))
+        g.close()
+    for f in fields:
+        f.close()
+    return {
+        "fields": len(specs),
+        "steps": args.ensemble_steps,
+        "size_classes": info["classes"],
+        "launches_per_step": info["launches_per_step"],
+        "seconds": el,
+        "grid_point_steps_per_s": gp / el,
+        "sequential_fp64_seconds": seq_s,
+        "sequential_fp64_grid_point_steps_per_s": gp / seq_s,
+        "speedup_vs_sequential_fp64": seq_s / el,
+        "eta_err_over_Hs_max_of_4_fp64_reruns": max(errs),
+        "timing": "wall clock of the graph launches with a device sync at both ends",
+    }
+
+
+def run_serving(args, capacity_gps):
+    from hos_b200.serve import Server, poisson_requests
+
+    nominal = poisson_requests(200.0, 10.0, seed=3)
+    offered = sum(r.n * r.n * r.steps for r in nominal) / 10.0
+    reqs = poisson_requests(args.serve_rate, args.serve_duration, seed=4)
+    m = Server(chunk=25).run(reqs, realtime=True, time_limit=args.serve_limit)
+    m.update({
+        "arrival_rate_per_s": args.serve_rate,
+        "arrival_window_s": args.serve_duration,
+        "request_mix": "grid uniform over 64^2..2048^2 (powers of two), M in 3..6, steps uniform in [100, 2000], "
+                       "half finite depth kp*h in [1,3], FP32 compute / FP64 state",
+        "nominal_stream": {"rate_per_s": 200.0, "window_s": 10.0, "requests": len(nominal),
+                           "offered_grid_point_steps_per_s": offered,
+                           "offered_over_capacity": offered / capacity_gps if capacity_gps else None},
+        "vs_sequential_fp64": None,
+    })
+    return m
+
+
 # ------------------------------------------------------------------ reference arm
 def run_reference(args, rank, world):
     if rank != 0:
@@ -270,7 +384,7 @@ def run_ours(args, rank, world, local_rank):
         return float(t.item())
 
     eta, phi, info, dt, desc = workload(args.n, args.order, seed=1000 + rank)
-    fields = {p: HosField(args.n, args.n, order=args.order, precision=p) for p in ("fp64", "fp32")}
+    fields = {p: HosField(args.n, args.n, order=args.order, precision=p, tune="auto") for p in ("fp64", "fp32")}
     for f in fields.values():
         f.set_state_physical(eta, phi)
     clocks = Clocks(local_rank)
@@ -402,6 +516,12 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": args.steps * f.launches_per_step,
         "clocks": clk,
     }
+    if not args.no_ensemble:
+        ens = run_ensemble(args, seed=rank)
+        line["ensemble"] = ens
+        srv = run_serving(args, ens["grid_point_steps_per_s"])
+        srv["vs_sequential_fp64"] = srv["grid_point_steps_per_s"] / ens["sequential_fp64_grid_point_steps_per_s"]
+        line["serving"] = srv
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
         cb = cpu_reference_rate(args, eta, phi, info, dt, max_seconds=20.0)

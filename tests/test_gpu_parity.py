@@ -264,3 +264,16 @@ def test_energy_conserved_1024_m5():
         f.step(info["Tp"] / 50, 200)
         _, H = f.energy_history()
     assert abs(H[-1] - H[0]) / abs(H[0]) < 1e-3
+
+
+def test_one_step_2048_vs_reference():
+    """The largest grid of the serving mix, one RK4 step, M = 3."""
+    n = 2048
+    eta, phi, info = ic.jonswap(n, n, kp=128.0, steepness=0.08, seed=9)
+    dt = info["Tp"] / 50
+    ref_u, ref_h = _reference_steps(3, n, eta, phi, dt, 1)
+    with HosField(n, n, order=3) as f:
+        f.set_state_physical(eta, phi)
+        f.step(dt, 1)
+        u, _ = f.state_spectral()
+    assert rel(u[0], ref_u[0]) < TOL_STEPS and rel(u[1], ref_u[1]) < TOL_STEPS
