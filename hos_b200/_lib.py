@@ -45,6 +45,7 @@ class HosParams(ctypes.Structure):
         ("mx", ctypes.c_int),
         ("my", ctypes.c_int),
         ("tune", ctypes.c_int * 8),
+        ("tune_opb", ctypes.c_int),
     ]
 
 

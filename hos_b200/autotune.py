@@ -1,12 +1,13 @@
 """Autotuner of the kernel shapes (elements per thread E and lines per block)
-of the four pass kinds, per grid, order and precision.
+of the four pass kinds, and of the z-derivative orders per block of the
+level x-forward pass, per grid, order and precision.
 
 Each pass kind (x-inverse, x-forward, y-inverse, y-forward) is tuned on its
 own: for every candidate (E, lines-per-block scale) a handle is created with
 that shape for the kind and defaults for the rest, a seeded sea is loaded,
 and the kind's passes of one RK stage are timed with CUDA events on the
 handle's stream (hos_profile_stage).  The fastest shape of each kind wins;
-the result (the 8 ``hos_params.tune`` values) is cached in a JSON file keyed
+the result (the 8 ``hos_params.tune`` values and ``tune_opb``) is cached in a JSON file keyed
 by GPU name, grid, order and precision (``HOS_AUTOTUNE_CACHE``, default
 ``~/.cache/hos_b200/autotune.json``).
 """
@@ -64,8 +65,8 @@ def _kind_ms(field, dt, names, reps):
 
 
 def tune(nx, ny, order=5, precision="fp32", reps=5, use_cache=True, scales=(-1, 0, 1)):
-    """Return the 8 tune values for (nx, ny, order, precision), measuring and
-    caching them if needed."""
+    """Return the 9 tune values (8 shapes, then orders per block) for
+    (nx, ny, order, precision), measuring and caching them if needed."""
     from . import ic
     from .field import HosField
 
@@ -76,33 +77,35 @@ def tune(nx, ny, order=5, precision="fp32", reps=5, use_cache=True, scales=(-1, 
     kp = max(2.0, min(nx, ny) / 42.0)
     eta, phi, info = ic.jonswap(nx, ny, kp=kp, steepness=0.08, seed=123)
     dt = info["Tp"] / 50
-    best = [0] * 8
+    best = [0] * 9
     report = {}
     failed = []
     for kind, (ie, isc, names) in KINDS.items():
         n = nx if kind[0] == "x" else ny // 2
         results = []
-        for e in _valid_elems(precision, n):
-            for s in scales:
-                t = [0] * 8
-                t[ie], t[isc] = e, s
-                try:
-                    f = HosField(nx, ny, order=order, precision=precision, tune=t)
-                except Exception:
-                    continue
-                try:
-                    f.set_state_physical(eta, phi)
-                    f.step(dt, 2)
-                    f.sync()
-                    results.append((_kind_ms(f, dt, names, reps), e, s))
-                except Exception as ex:  # a shape this device cannot launch: skip it
-                    failed.append({"kind": kind, "E": e, "scale": s, "error": str(ex)})
-                finally:
-                    f.close()
+        opbs = (1, 2, order) if kind == "xf" else (0,)
+        for e, s, ob in [(e, s, ob) for e in _valid_elems(precision, n) for s in scales for ob in opbs]:
+            t = [0] * 9
+            t[ie], t[isc], t[8] = e, s, ob
+            try:
+                f = HosField(nx, ny, order=order, precision=precision, tune=t)
+            except Exception:
+                continue
+            try:
+                f.set_state_physical(eta, phi)
+                f.step(dt, 2)
+                f.sync()
+                results.append((_kind_ms(f, dt, names, reps), e, s, ob))
+            except Exception as ex:  # a shape this device cannot launch: skip it
+                failed.append({"kind": kind, "E": e, "scale": s, "opb": ob, "error": str(ex)})
+            finally:
+                f.close()
         if results:
-            ms, e, s = min(results)
+            ms, e, s, ob = min(results)
             best[ie], best[isc] = e, s
-            report[kind] = {"E": e, "scale": s, "ms": ms, "tried": len(results)}
+            if kind == "xf":
+                best[8] = ob
+            report[kind] = {"E": e, "scale": s, "opb": ob, "ms": ms, "tried": len(results)}
     if use_cache:
         db = _load()
         db[key] = {"tune": best, "report": report, "failed": failed}

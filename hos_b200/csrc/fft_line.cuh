@@ -275,10 +275,27 @@ __device__ __forceinline__ void line_fft(cpx<T> (&v)[E], cpx<T>* sm, int t, cons
 #pragma unroll
   for (int s = 0; s < SF; s++) {
     if (s > 0) {
+      // twiddles w^r, w = exp(-+2 pi i jm/(ns E)): the powers w^(2^b) come
+      // from the table and every other power is a product of those, so each
+      // twiddle is at most log2(E)-1 products away from a table value
       const int jm = t & (ns - 1);
       const int scale = N / (ns * E);
+      C wp[LP::LOGE];
 #pragma unroll
-      for (int r = 1; r < E; r++) v[r] = cmul(v[r], twid<INV>(tw, r * jm, scale));
+      for (int b = 0; b < LP::LOGE; b++) wp[b] = twid<INV>(tw, (1 << b) * jm, scale);
+#pragma unroll
+      for (int r = 1; r < E; r++) {
+        C w;
+        bool first = true;
+#pragma unroll
+        for (int b = 0; b < LP::LOGE; b++) {
+          if (r & (1 << b)) {
+            w = first ? wp[b] : cmul(w, wp[b]);
+            first = false;
+          }
+        }
+        v[r] = cmul(v[r], w);
+      }
     }
     dft<E, INV>(v);
     const bool last = (s == SF - 1) && (RL == 1);

@@ -238,6 +238,7 @@ namespace {
 struct ElemChoice {
   int xi = 8, xf = 8, yi = 8, yf = 8;          // elements per thread
   int sxi = 0, sxf = 0, syi = 0, syf = 0;      // lines per block scaled by 2^s
+  int opb = 1;                                 // z-derivative orders per block of the level x-forward pass
 };
 
 // Launch geometry of one pass kind: elements per thread E, lines per block,
@@ -685,10 +686,13 @@ void build_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, doub
     r4.kind = L_XFWD;
     r4.mode = XF_LEVEL;
     r4.gx = xgrid(c, g.xf);
-    r4.gy = M - n;
+    const int opb = c->cfg.ec.opb > 0 ? c->cfg.ec.opb : 1;
+    r4.gy = (M - n + opb - 1) / opb;
     XFwdArgs& xf = r4.xf;
     xf.geo = c->geo;
-    xf.ycount = M - n;
+    xf.ycount = r4.gy;
+    xf.ndz = M - n;
+    xf.opb = opb;
     xf.rows = c->h + 1;
     xf.vin0 = zb;
     xf.zout = zb + fsz * cs;
@@ -983,7 +987,8 @@ bool same_class(const hos_ctx* a, const hos_ctx* b) {
   return a->nx == b->nx && a->ny == b->ny && a->prec == b->prec && a->p.scheme == b->p.scheme &&
          a->cfg.ec.xi == b->cfg.ec.xi && a->cfg.ec.xf == b->cfg.ec.xf && a->cfg.ec.yi == b->cfg.ec.yi &&
          a->cfg.ec.yf == b->cfg.ec.yf && a->cfg.ec.sxi == b->cfg.ec.sxi && a->cfg.ec.sxf == b->cfg.ec.sxf &&
-         a->cfg.ec.syi == b->cfg.ec.syi && a->cfg.ec.syf == b->cfg.ec.syf && a->device == b->device;
+         a->cfg.ec.syi == b->cfg.ec.syi && a->cfg.ec.syf == b->cfg.ec.syf && a->cfg.ec.opb == b->cfg.ec.opb &&
+         a->device == b->device;
 }
 
 // Slot of the r-th pass of a member with L levels in a class whose deepest
@@ -1268,6 +1273,7 @@ int hos_create(const hos_params* p, hos_handle* out) {
     ec.sxf = clamp3(p->tune[5]);
     ec.syi = clamp3(p->tune[6]);
     ec.syf = clamp3(p->tune[7]);
+    if (p->tune_opb > 0) ec.opb = p->tune_opb;
     rc = make_cfg(c, c->prec, ec, &c->cfg);
     if (!rc) rc = make_cfg(c, 0, ec64, &c->cfg64);
   }

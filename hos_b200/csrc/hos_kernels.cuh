@@ -173,7 +173,9 @@ struct XFwdArgs {
   int dealias;          // PLAIN: zero the modes Dealias zeroes (operators_par.c:283-325)
   int addk_mask;        // PLAIN: bit q set -> add Dz of the phi field of u_add to output q (W^(1), hosm_2d_par.c:280-288)
   const double2* u_add; // PLAIN: packed state whose phi field supplies that term
-  void* zout;           // LEVEL: output Z arrays (T2), stride (h+1)*nx; order blockIdx.y+1
+  void* zout;           // LEVEL: output Z arrays (T2), stride (h+1)*nx
+  int ndz;              // LEVEL: z-derivative orders 1..ndz
+  int opb;              // LEVEL: orders per block (blockIdx.y covers orders y*opb+1 ..)
   // RHS
   double2* u;                     // packed state at step start (updated in place on the final stage)
   const double2* ustg;            // stage input of both fields, written by the x-inverse pass
@@ -239,21 +241,25 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_xfwd(const __grid_constant__
       }
       return;
     }
-    // LEVEL: v holds phi^(n+1) hat; this block emits its z-derivative of
-    // order p = blockIdx.y + 1 (the forward transform is repeated per order
-    // so that the orders run in parallel blocks)
+    // LEVEL: v holds phi^(n+1) hat; this block emits its z-derivatives of
+    // orders p0+1 .. p0+opb, p0 = blockIdx.y*opb (the forward transform is
+    // repeated per block, so opb trades repeated work for parallel blocks)
     const double ky = ky_of(geo, row);
-    const int p = blockIdx.y + 1;
-    C* z = reinterpret_cast<C*>(a.zout) + (size_t)(p - 1) * fsz;
+    const int p0 = blockIdx.y * a.opb;
+    const int p1 = min(p0 + a.opb, a.ndz);
+    for (int p = p0 + 1; p <= p1; p++) {
+      C w[E];
 #pragma unroll
-    for (int e = 0; e < E; e++) {
-      const double kx = kx_of(geo, t + e * P);
-      v[e] = cscale(v[e], (T)dz_mult(geo, sqrt(kx * kx + ky * ky), p));
-    }
-    line_fft<T, NX, E, true>(v, sm, t, tw);
-    if (live) {
+      for (int e = 0; e < E; e++) {
+        const double kx = kx_of(geo, t + e * P);
+        w[e] = cscale(v[e], (T)dz_mult(geo, sqrt(kx * kx + ky * ky), p));
+      }
+      line_fft<T, NX, E, true>(w, sm, t, tw);
+      if (live) {
+        C* z = reinterpret_cast<C*>(a.zout) + (size_t)(p - 1) * fsz;
 #pragma unroll
-      for (int e = 0; e < E; e++) z[roff + t + e * P] = v[e];
+        for (int e = 0; e < E; e++) z[roff + t + e * P] = w[e];
+      }
     }
     return;
   }

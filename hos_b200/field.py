@@ -74,8 +74,11 @@ class HosField:
             tune = _autotune(int(nx), int(ny), int(order), precision if isinstance(precision, str) else
                              ("fp32" if int(precision) else "fp64"))
         if tune is not None:
-            for i, v in enumerate(list(tune)[:8]):
+            tv = list(tune)
+            for i, v in enumerate(tv[:8]):
                 p.tune[i] = int(v)
+            if len(tv) > 8:
+                p.tune_opb = int(tv[8])
         self.params = p
         self.nx, self.ny, self.h = int(nx), int(ny), int(ny) // 2
         h = ctypes.c_void_p()
