@@ -46,6 +46,7 @@ class HosParams(ctypes.Structure):
         ("my", ctypes.c_int),
         ("tune", ctypes.c_int * 8),
         ("tune_opb", ctypes.c_int),
+        ("tune_nofuse", ctypes.c_int),
     ]
 
 

@@ -24,6 +24,7 @@
 #include <mutex>
 #include <string>
 #include <algorithm>
+#include <map>
 #include <vector>
 
 #include "hos_gpu.h"
@@ -239,6 +240,7 @@ struct ElemChoice {
   int xi = 8, xf = 8, yi = 8, yf = 8;          // elements per thread
   int sxi = 0, sxf = 0, syi = 0, syf = 0;      // lines per block scaled by 2^s
   int opb = 1;                                 // z-derivative orders per block of the level x-forward pass
+  int fuse = 1;                                // next level's y-forward inside each level's y-inverse
 };
 
 // Launch geometry of one pass kind: elements per thread E, lines per block,
@@ -582,6 +584,7 @@ void log_pass(hos_ctx* c, PassLog* lg, int kind, double bytes) {
 enum LaunchKind { L_XINV, L_XFWD, L_YINV, L_YFWD };
 struct PassRec {
   int kind = 0, mode = 0;
+  int slot = 0;        // position in the stage, shared by the same pass of every member of an ensemble
   int gx = 1, gy = 1;  // grid (x: rows or x-row groups, y: outputs)
   int log_kind = 0;    // PassKind for the per-pass profile
   double bytes = 0.0;  // algorithmic bytes of the launch
@@ -634,6 +637,7 @@ void build_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, doub
   xa.set_ramp = (s == 0);
   xa.tramp = c->p.tramp;
   xa.rampflg = c->p.rampflg;
+  r1.slot = 0;
   r1.log_kind = P_XINV_STAGE;
   r1.bytes = act * nxd * (16.0 * 2 * (1 + nk) + (double)cs * (4 + M));
   out.push_back(r1);
@@ -658,11 +662,14 @@ void build_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, doub
   for (int j = 1; j <= M; j++) ya.jobs[nj++] = YJob{4 + j - 1, 0, c->D(1, j)};
   ya.ycount = nj;
   r2.gy = nj;
+  r2.slot = 1;
   r2.log_kind = P_YINV_STAGE;
   r2.bytes = act * nxd * (double)cs * (4 + M) + psz * (double)rs * (5 + M);
   out.push_back(r2);
 
   for (int n = 1; n <= L; n++) {
+    const bool fused_in = c->cfg.ec.fuse && n >= 2;  // this level's y-forward ran inside level n-1's y-inverse
+    if (!fused_in) {
     PassRec r3;
     r3.kind = L_YFWD;
     r3.mode = YF_LEVEL;
@@ -678,9 +685,11 @@ void build_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, doub
     for (int p = 1; p <= n; p++) fa.t_in[p - 1] = c->D(n - p + 1, p);  // power p: m = n - p
     fa.vout = zb;
     fa.rows_out = c->h + 1;
+    r3.slot = 2 + 3 * (n - 1);
     r3.log_kind = P_YFWD_LEVEL;
     r3.bytes = psz * (double)rs * (n + 1) + fszd * (double)cs;
     out.push_back(r3);
+    }
 
     PassRec r4;
     r4.kind = L_XFWD;
@@ -696,6 +705,7 @@ void build_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, doub
     xf.rows = c->h + 1;
     xf.vin0 = zb;
     xf.zout = zb + fsz * cs;
+    r4.slot = 3 + 3 * (n - 1);
     r4.log_kind = P_XFWD_LEVEL;
     r4.bytes = fszd * (double)cs * (1 + M - n);
     out.push_back(r4);
@@ -718,8 +728,20 @@ void build_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, doub
     yl.eta = c->ETA();
     yl.w_terms = n;
     for (int p = 1; p <= n; p++) yl.w_in[p - 1] = c->D(n - p + 1, p + 1);  // power p: m = n - p
+    yl.store_job0 = 1;
+    r5.slot = 4 + 3 * (n - 1);
     r5.log_kind = P_YINV_LEVEL;
     r5.bytes = fszd * (double)cs * (M - n) + psz * (double)rs * (M - n + 1 + n + 1);
+    if (c->cfg.ec.fuse && n < L) {
+      // the next level's P_(n+1) and its y-forward transform in the job-0 blocks;
+      // d_z phi^(n+1) (job 0) then has no other reader and is not stored
+      yl.fuse_next = 1;
+      yl.nx_terms = n + 1;
+      for (int p = 2; p <= n + 1; p++) yl.nx_in[p - 1] = c->D(n + 2 - p, p);
+      yl.vout = zb;
+      yl.store_job0 = 0;
+      r5.bytes += psz * (double)rs * (n - 1) + fszd * (double)cs;
+    }
     out.push_back(r5);
   }
 
@@ -743,6 +765,7 @@ void build_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, doub
     zf.which_base = 2;
     zf.vout = zb;
     zf.rows_out = c->h + 1;
+    rz.slot = 100;
     out.push_back(rz);
     PassRec rx;
     rx.kind = L_XFWD;
@@ -757,6 +780,7 @@ void build_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, doub
     xz.out_spec = zvel_out;
     xz.addk_mask = 1 | (L >= 2 ? 2 : 0);  // W^(1) belongs to W^(M) always and to W^(M-2) when L >= 2
     xz.u_add = uin;
+    rx.slot = 101;
     out.push_back(rx);
     return;
   }
@@ -779,6 +803,7 @@ void build_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, doub
   for (int n = 0; n <= L; n++) ff.w_idx[n] = c->W(n);
   ff.vout = zb;
   ff.rows_out = c->geo.my;
+  r6.slot = 100;
   r6.log_kind = P_YFWD_RHS;
   r6.bytes = psz * (double)rs * (5 + L) + 2.0 * my * nxd * (double)cs;
   out.push_back(r6);
@@ -812,6 +837,7 @@ void build_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, doub
   // stage also the other k's and the updated u (rows < my)
   double b = 2.0 * my * nxd * (double)cs + act * nxd * 16.0 * 2 + my * nxd * 16.0 * 2;
   if (xe.final_update) b += my * nxd * 16.0 * 2 * (c->nst - 1) + my * nxd * 16.0 * 2;
+  r7.slot = 101;
   r7.log_kind = P_XFWD_RHS;
   r7.bytes = b;
   out.push_back(r7);
@@ -987,15 +1013,8 @@ bool same_class(const hos_ctx* a, const hos_ctx* b) {
   return a->nx == b->nx && a->ny == b->ny && a->prec == b->prec && a->p.scheme == b->p.scheme &&
          a->cfg.ec.xi == b->cfg.ec.xi && a->cfg.ec.xf == b->cfg.ec.xf && a->cfg.ec.yi == b->cfg.ec.yi &&
          a->cfg.ec.yf == b->cfg.ec.yf && a->cfg.ec.sxi == b->cfg.ec.sxi && a->cfg.ec.sxf == b->cfg.ec.sxf &&
-         a->cfg.ec.syi == b->cfg.ec.syi && a->cfg.ec.syf == b->cfg.ec.syf && a->cfg.ec.opb == b->cfg.ec.opb &&
+         a->cfg.ec.syi == b->cfg.ec.syi && a->cfg.ec.syf == b->cfg.ec.syf && a->cfg.ec.opb == b->cfg.ec.opb && a->cfg.ec.fuse == b->cfg.ec.fuse &&
          a->device == b->device;
-}
-
-// Slot of the r-th pass of a member with L levels in a class whose deepest
-// member has Lmax levels: K1, K2, 3 per level, then the two RHS passes.
-int slot_of(int r, int L, int Lmax, int npass) {
-  if (r < 2 + 3 * L) return r;
-  return 2 + 3 * Lmax + (r - (npass - 2));
 }
 
 struct BatchLaunch {
@@ -1005,8 +1024,8 @@ struct BatchLaunch {
 
 // Builds the launches of one RK step of an ensemble and the host image of
 // their argument arrays.
-void plan_step(hos_ens* E, std::vector<std::vector<BatchLaunch>>& per_class, std::vector<unsigned char>& img,
-               std::vector<StepEndArgs>& ends, std::vector<size_t>& end_off) {
+int plan_step(hos_ens* E, std::vector<std::vector<BatchLaunch>>& per_class, std::vector<unsigned char>& img,
+              std::vector<StepEndArgs>& ends, std::vector<size_t>& end_off) {
   per_class.assign(E->cls.size(), {});
   auto put = [&](const void* p, size_t n) {
     size_t off = (img.size() + 255) & ~(size_t)255;
@@ -1017,20 +1036,20 @@ void plan_step(hos_ens* E, std::vector<std::vector<BatchLaunch>>& per_class, std
   for (size_t ci = 0; ci < E->cls.size(); ci++) {
     const EnsClass& K = E->cls[ci];
     const int nst = E->mem[K.idx[0]]->nst;
-    int Lmax = 0;
-    for (int f : K.idx) Lmax = std::max(Lmax, E->mem[f]->L);
-    const int nslot = 2 + 3 * Lmax + 2;
     for (int s = 0; s < nst; s++) {
-      std::vector<std::vector<PassRec>> bys(nslot);
+      std::map<int, std::vector<PassRec>> bys;  // slot -> the members' records, in slot order
       for (int f : K.idx) {
         hos_ctx* c = E->mem[f];
         std::vector<PassRec> recs;
         build_stage(c, s, E->dt[f], false, c->u, c->k + (size_t)s * 2 * c->fsz, c->tdev, c->actdev, nullptr, 0, recs);
-        for (size_t r = 0; r < recs.size(); r++) bys[slot_of((int)r, c->L, Lmax, (int)recs.size())].push_back(recs[r]);
+        for (const PassRec& r : recs) bys[r.slot].push_back(r);
       }
-      for (int sl = 0; sl < nslot; sl++) {
-        const std::vector<PassRec>& v = bys[sl];
+      for (const auto& kv : bys) {
+        const std::vector<PassRec>& v = kv.second;
         if (v.empty()) continue;
+        for (const PassRec& r : v)  // one launch runs one kernel: every record must be of that kernel
+          if (r.kind != v[0].kind || r.mode != v[0].mode || r.gx != v[0].gx)
+            return fail(HOS_ERR_STATE, "ensemble plan: members disagree at pass slot %d", kv.first);
         BatchLaunch b;
         b.kind = v[0].kind;
         b.mode = v[0].mode;
@@ -1067,6 +1086,7 @@ void plan_step(hos_ens* E, std::vector<std::vector<BatchLaunch>>& per_class, std
     end_off.push_back(put(se.data(), se.size() * sizeof(StepEndArgs)));
     ends.insert(ends.end(), se.begin(), se.end());
   }
+  return HOS_OK;
 }
 
 int build_ens_graph(hos_ens* E) {
@@ -1074,7 +1094,8 @@ int build_ens_graph(hos_ens* E) {
   std::vector<unsigned char> img;
   std::vector<StepEndArgs> ends;
   std::vector<size_t> end_off;
-  plan_step(E, per_class, img, ends, end_off);
+  int prc = plan_step(E, per_class, img, ends, end_off);
+  if (prc) return prc;
   if (img.size() > E->dargs_bytes) {
     if (E->dargs) cudaFree(E->dargs);
     E->dargs = nullptr;
@@ -1274,6 +1295,7 @@ int hos_create(const hos_params* p, hos_handle* out) {
     ec.syi = clamp3(p->tune[6]);
     ec.syf = clamp3(p->tune[7]);
     if (p->tune_opb > 0) ec.opb = p->tune_opb;
+    if (p->tune_nofuse) ec.fuse = 0;
     rc = make_cfg(c, c->prec, ec, &c->cfg);
     if (!rc) rc = make_cfg(c, 0, ec64, &c->cfg64);
   }
@@ -1696,7 +1718,8 @@ int hos_ensemble_destroy(hos_ensemble e) {
 
 int hos_launches_per_step(hos_handle h) {
   if (!h) return -1;
-  return h->nst * (4 + 3 * h->L) + 1;
+  const int per_stage = 4 + 3 * h->L - (h->cfg.ec.fuse && h->L >= 2 ? h->L - 1 : 0);
+  return h->nst * per_stage + 1;
 }
 
 int hos_volume(hos_handle h, double* vol) {

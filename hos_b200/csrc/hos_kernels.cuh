@@ -62,6 +62,26 @@ __device__ __forceinline__ double dz_mult(const Geo& G, double kz, int p) {
   return m;
 }
 
+// The same multiplier at the compute precision T of a pass: in single
+// precision it only scales single-precision data, so it is formed in single
+// precision too (kx, ky and the quirky kx convention as in kx_of).
+template <typename T>
+__device__ __forceinline__ T dz_mult_t(const Geo& G, int i, int j, int p);
+template <>
+__device__ __forceinline__ double dz_mult_t<double>(const Geo& G, int i, int j, int p) {
+  const double kx = kx_of(G, i), ky = ky_of(G, j);
+  return dz_mult(G, sqrt(kx * kx + ky * ky), p);
+}
+template <>
+__device__ __forceinline__ float dz_mult_t<float>(const Geo& G, int i, int j, int p) {
+  const float kx = (float)kx_of(G, i), ky = (float)ky_of(G, j);
+  const float kz = sqrtf(kx * kx + ky * ky);
+  float m = 1.0f;
+  for (int q = 0; q < p; q++) m *= kz;
+  if ((p & 1) && G.depth > 0) m *= tanhf(kz * (float)G.depth);
+  return m;
+}
+
 enum { XI_STAGE = 0, XI_PLAIN = 1 };
 enum { XF_PLAIN = 0, XF_LEVEL = 1, XF_RHS = 2 };
 enum { YI_JOBS = 0, YI_LEVEL = 1 };
@@ -127,7 +147,6 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_xinv(const __grid_constant__
     for (int e = 0; e < E; e++) v[e] = live ? conv<T>(a.u[roff + t + e * P]) : mkc((T)0, (T)0);
   } else {
     const size_t foff = (o < 2) ? 0 : fsz;
-    const double ky = ky_of(geo, row);
 #pragma unroll
     for (int e = 0; e < E; e++) {
       double2 x = make_double2(0.0, 0.0);
@@ -145,12 +164,12 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_xinv(const __grid_constant__
       if (o == 1 || o == 3) {  // Dx: i kx (operators_par.c:66)
         const double kx = kx_of(geo, i);
         x = make_double2(-kx * x.y, kx * x.x);
+        v[e] = conv<T>(x);
       } else if (o >= 4) {  // Dz applied o-3 times (operators_par.c:168-192)
-        const double kx = kx_of(geo, i);
-        const double m = dz_mult(geo, sqrt(kx * kx + ky * ky), o - 3);
-        x = make_double2(m * x.x, m * x.y);
+        v[e] = cscale(conv<T>(x), dz_mult_t<T>(geo, i, row, o - 3));
+      } else {
+        v[e] = conv<T>(x);
       }
-      v[e] = conv<T>(x);
     }
   }
   line_fft<T, NX, E, true>(v, sm, t, tw);
@@ -244,16 +263,12 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_xfwd(const __grid_constant__
     // LEVEL: v holds phi^(n+1) hat; this block emits its z-derivatives of
     // orders p0+1 .. p0+opb, p0 = blockIdx.y*opb (the forward transform is
     // repeated per block, so opb trades repeated work for parallel blocks)
-    const double ky = ky_of(geo, row);
     const int p0 = blockIdx.y * a.opb;
     const int p1 = min(p0 + a.opb, a.ndz);
     for (int p = p0 + 1; p <= p1; p++) {
       C w[E];
 #pragma unroll
-      for (int e = 0; e < E; e++) {
-        const double kx = kx_of(geo, t + e * P);
-        w[e] = cscale(v[e], (T)dz_mult(geo, sqrt(kx * kx + ky * ky), p));
-      }
+      for (int e = 0; e < E; e++) w[e] = cscale(v[e], dz_mult_t<T>(geo, t + e * P, row, p));
       line_fft<T, NX, E, true>(w, sm, t, tw);
       if (live) {
         C* z = reinterpret_cast<C*>(a.zout) + (size_t)(p - 1) * fsz;
@@ -339,6 +354,55 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_xfwd(const __grid_constant__
   }
 }
 
+// Forward y-transform of the values v (pairs of physical points of this
+// thread's line), real-to-complex postprocessing, and the transposed store of
+// rows ky < rows_out of the G lines into the [h+1][nx] array vo.  All threads
+// of the block must call it.
+template <typename T, int H, int E>
+__device__ __forceinline__ void yfwd_finish(cpx<T> (&v)[E], cpx<T>* sm, cpx<T>* tl, int t, int G, int lp,
+                                            const cpx<T>* tw, const cpx<T>* twy, cpx<T>* vo, int nx, int ix0,
+                                            int rows_out) {
+  using C = cpx<T>;
+  constexpr int P = H / E;
+  line_fft<T, H, E, false>(v, tl, t, tw);
+  // C[k] natural order -> line region, then real-to-complex postprocessing in
+  // place, one (k, H-k) pair per thread slot
+  __syncthreads();
+#pragma unroll
+  for (int e = 0; e < E; e++) tl[(t + e * P)] = v[e];
+  __syncthreads();
+#pragma unroll
+  for (int e = 0; e <= E / 2; e++) {
+    int k;
+    if (e < E / 2) k = t + e * P;  // pairs (k, H-k), k in [0, H/2)
+    else if (t == 0) k = H / 2;    // the self-paired middle bin
+    else break;
+    const int kn = H - k;  // partner; for k = 0 the partner is the Nyquist bin H (C[H] = C[0])
+    const C ck = tl[(k)];
+    const C cq = tl[(kn & (H - 1))];
+    // X[k] = (C[k] + conj C[H-k])/2 + w^k (C[k] - conj C[H-k])/(2i),  w = exp(-2 pi i / Ny)
+    const C cn = cconj(cq);
+    const C ev = cscale(cadd(ck, cn), (T)0.5);
+    const C d = csub(ck, cn);
+    const C od = mkc((T)0.5 * d.y, (T)-0.5 * d.x);
+    const C xk = cadd(ev, cmul(__ldg(&twy[k]), od));
+    if (k != kn) {
+      const C cm = cconj(ck);
+      const C ev2 = cscale(cadd(cq, cm), (T)0.5);
+      const C d2 = csub(cq, cm);
+      const C od2 = mkc((T)0.5 * d2.y, (T)-0.5 * d2.x);
+      tl[(kn)] = cadd(ev2, cmul(__ldg(&twy[kn]), od2));
+    }
+    tl[(k)] = xk;
+  }
+  __syncthreads();
+  const int ntot = G * rows_out;
+  for (int q = threadIdx.x; q < ntot; q += blockDim.x) {
+    const int ky = q / G, g = q - ky * G;
+    vo[(size_t)ky * nx + ix0 + g] = sm[(size_t)g * lp + (ky)];
+  }
+}
+
 // ---------------------------------------------------------------- y passes
 // Shared memory of a y-pass block: G line regions of `lp` complex elements.
 // A line region first holds the line's spectral column (index ky) and then
@@ -367,6 +431,14 @@ struct YInvArgs {
   int eta;
   int w_terms;
   int w_in[MAX_TERMS];
+  // LEVEL, fused with the next level's y-forward pass: the job-0 block also
+  // forms P_(n+1) = -sum_p phys[nx_in[p-1]] eta^p/p! with the p = 1 term taken
+  // from its own result (not stored), transforms it along y and writes V.
+  int fuse_next;
+  int nx_terms;
+  int nx_in[MAX_TERMS];
+  void* vout;
+  int store_job0;  // 0 when the fused job-0 result has no other reader
 };
 
 template <typename T, int H, int E, int MODE, bool B>
@@ -431,17 +503,21 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yinv(const __grid_constant__
   line_fft<T, H, E, true>(v, tl, t, tw);  // starts with a barrier before reusing tl
   // v[e] holds (x[2m], x[2m+1]) for m = t + e*P of physical row ix
   C* po = reinterpret_cast<C*>(pall + (size_t)J.out * psz + (size_t)ix * ny);
+  if (MODE != YI_LEVEL || blockIdx.y != 0 || a.store_job0) {
 #pragma unroll
-  for (int e = 0; e < E; e++) po[t + e * P] = v[e];
+    for (int e = 0; e < E; e++) po[t + e * P] = v[e];
+  }
   if (MODE == YI_LEVEL && blockIdx.y == 0) {
     // terms ordered by power 1, 2, ..., w_terms (host side); p = eta^k/k!
     const C* pe = reinterpret_cast<const C*>(pall + (size_t)a.eta * psz + (size_t)ix * ny);
     C* pwo = reinterpret_cast<C*>(pall + (size_t)a.w_out * psz + (size_t)ix * ny);
     C et[E], p[E];
+    C own[E];  // this block's result, d_z phi^(n+1)
 #pragma unroll
     for (int e = 0; e < E; e++) {
       et[e] = pe[t + e * P];
       p[e] = mkc((T)1, (T)1);
+      own[e] = v[e];
     }
     for (int q = 0; q < a.w_terms; q++) {
       const C* pd = reinterpret_cast<const C*>(pall + (size_t)a.w_in[q] * psz + (size_t)ix * ny);
@@ -457,7 +533,30 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yinv(const __grid_constant__
     }
 #pragma unroll
     for (int e = 0; e < E; e++) pwo[t + e * P] = v[e];
+    if (a.fuse_next) {
+      // P_(n+1) (hosm_2d_par.c:302-317): the power-1 term is own * eta
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        p[e] = et[e];
+        v[e].x = -own[e].x * et[e].x;
+        v[e].y = -own[e].y * et[e].y;
+      }
+      for (int q = 1; q < a.nx_terms; q++) {
+        const C* pd = reinterpret_cast<const C*>(pall + (size_t)a.nx_in[q] * psz + (size_t)ix * ny);
+        const T inv = (T)1 / (T)(q + 1);
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+          const C d = pd[t + e * P];
+          p[e].x = p[e].x * et[e].x * inv;
+          p[e].y = p[e].y * et[e].y * inv;
+          v[e].x -= d.x * p[e].x;
+          v[e].y -= d.y * p[e].y;
+        }
+      }
+    }
   }
+  if (MODE == YI_LEVEL && a.fuse_next && blockIdx.y == 0)
+    yfwd_finish<T, H, E>(v, sm, tl, t, G, a.lp, tw, twy, reinterpret_cast<C*>(a.vout), nx, ix0, H + 1);
 }
 
 struct YFwdArgs {
@@ -596,44 +695,8 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yfwd(const __grid_constant__
     }
   }
 
-  line_fft<T, H, E, false>(v, tl, t, tw);
-  // C[k] natural order -> line region, then real-to-complex postprocessing in
-  // place, one (k, H-k) pair per thread slot
-  __syncthreads();
-#pragma unroll
-  for (int e = 0; e < E; e++) tl[(t + e * P)] = v[e];
-  __syncthreads();
-#pragma unroll
-  for (int e = 0; e <= E / 2; e++) {
-    int k;
-    if (e < E / 2) k = t + e * P;  // pairs (k, H-k), k in [0, H/2)
-    else if (t == 0) k = H / 2;    // the self-paired middle bin
-    else break;
-    const int kn = H - k;  // partner; for k = 0 the partner is the Nyquist bin H (C[H] = C[0])
-    const C ck = tl[(k)];
-    const C cq = tl[(kn & (H - 1))];
-    // X[k] = (C[k] + conj C[H-k])/2 + w^k (C[k] - conj C[H-k])/(2i),  w = exp(-2 pi i / Ny)
-    const C cn = cconj(cq);
-    const C ev = cscale(cadd(ck, cn), (T)0.5);
-    const C d = csub(ck, cn);
-    const C od = mkc((T)0.5 * d.y, (T)-0.5 * d.x);
-    const C xk = cadd(ev, cmul(__ldg(&twy[k]), od));
-    if (k != kn) {
-      const C cm = cconj(ck);
-      const C ev2 = cscale(cadd(cq, cm), (T)0.5);
-      const C d2 = csub(cq, cm);
-      const C od2 = mkc((T)0.5 * d2.y, (T)-0.5 * d2.x);
-      tl[(kn)] = cadd(ev2, cmul(__ldg(&twy[kn]), od2));
-    }
-    tl[(k)] = xk;
-  }
-  __syncthreads();
-  C* vo = reinterpret_cast<C*>(a.vout) + (size_t)blockIdx.y * fsz;
-  const int ntot = G * a.rows_out;
-  for (int q = threadIdx.x; q < ntot; q += blockDim.x) {
-    const int ky = q / G, g = q - ky * G;
-    vo[(size_t)ky * nx + ix0 + g] = sm[(size_t)g * a.lp + (ky)];
-  }
+  yfwd_finish<T, H, E>(v, sm, tl, t, G, a.lp, tw, twy, reinterpret_cast<C*>(a.vout) + (size_t)blockIdx.y * fsz, nx,
+                       ix0, a.rows_out);
 }
 
 }  // namespace hos

@@ -79,6 +79,8 @@ class HosField:
                 p.tune[i] = int(v)
             if len(tv) > 8:
                 p.tune_opb = int(tv[8])
+            if len(tv) > 9:
+                p.tune_nofuse = int(tv[9])
         self.params = p
         self.nx, self.ny, self.h = int(nx), int(ny), int(ny) // 2
         h = ctypes.c_void_p()

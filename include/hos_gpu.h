@@ -67,6 +67,8 @@ typedef struct hos_params {
                        y-inverse and y-forward passes (8, 16, or 32 in FP32), then the base-2 exponents
                        scaling their lines per block; chosen by hos_b200.autotune */
   int tune_opb;     /* z-derivative orders per block of the level x-forward pass (0 = 1) */
+  int tune_nofuse;  /* 1: run each level's y-forward pass as its own launch instead of inside the
+                       previous level's y-inverse pass */
 } hos_params;
 
 typedef struct hos_ctx* hos_handle;
