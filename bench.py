@@ -227,11 +227,16 @@ def run_ensemble(args, seed=0):
     ens.step(3)
     ens.sync()
     torch.cuda.synchronize()
-    stream = torch.cuda.ExternalStream(ens._lib.hos_stream(fields[0]._h))
+    stream = torch.cuda.ExternalStream(ens.stream)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
     t0 = time.perf_counter()
+    e0.record(stream)
     ens.step(args.ensemble_steps)
+    e1.record(stream)
     ens.sync()
-    el = time.perf_counter() - t0
+    wall = time.perf_counter() - t0
+    el = e0.elapsed_time(e1) / 1e3
     gp = sum(n * n for (n, *_r) in specs) * args.ensemble_steps
     info = ens.info
     ens.close()
@@ -246,10 +251,12 @@ def run_ensemble(args, seed=0):
             g._lib.hos_set_state_physical(g._h, _dptr(eta), _dptr(phi), 0.0)
             g.step(tp / 50, 3)
             g.sync()
-            t1 = time.perf_counter()
+            gs = torch.cuda.ExternalStream(g.stream)
+            e0.record(gs)
             g.step(tp / 50, 30)
+            e1.record(gs)
             g.sync()
-            rates[key] = (time.perf_counter() - t1) / 30
+            rates[key] = e0.elapsed_time(e1) / 1e3 / 30
             g.close()
         seq_s += rates[key] * args.ensemble_steps
     # accuracy of the FP32 members: four members rerun in FP64
@@ -277,7 +284,8 @@ def run_ensemble(args, seed=0):
         "sequential_fp64_grid_point_steps_per_s": gp / seq_s,
         "speedup_vs_sequential_fp64": seq_s / el,
         "eta_err_over_Hs_max_of_4_fp64_reruns": max(errs),
-        "timing": "wall clock of the graph launches with a device sync at both ends",
+        "wall_seconds": wall,
+        "timing": "CUDA events on the ensemble's stream around the step-graph launches",
     }
 
 
@@ -359,7 +367,7 @@ def run_reference(args, rank, world):
 
 
 # ------------------------------------------------------------------ our arm
-def run_ours(args, rank, world, local_rank):
+def run_ours(args, rep):
     import ctypes
 
     import numpy as np
@@ -367,23 +375,11 @@ def run_ours(args, rank, world, local_rank):
 
     from hos_b200 import HosField
 
+    rank, world, local_rank = rep.rank, rep.world, rep.local_rank
     torch.cuda.set_device(local_rank)
-    dist = world > 1
-    if dist:
-        import torch.distributed as tdist
+    barrier, max_over_ranks = rep.barrier, rep.max
 
-    def barrier():
-        if dist:
-            tdist.barrier()
-
-    def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        return float(t.item())
-
-    eta, phi, info, dt, desc = workload(args.n, args.order, seed=1000 + rank)
+    eta, phi, info, dt, desc = workload(args.n, args.order, seed=rep.seed(1000))
     fields = {p: HosField(args.n, args.n, order=args.order, precision=p, tune="auto") for p in ("fp64", "fp32")}
     for f in fields.values():
         f.set_state_physical(eta, phi)
@@ -548,21 +544,10 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
-    if world > 1:
-        import datetime
+    from hos_b200.replicas import Replicas
 
-        import torch
-        import torch.distributed as tdist
-
-        torch.cuda.set_device(local_rank)
-        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    try:
-        run_ours(args, rank, world, local_rank)
-    finally:
-        if world > 1:
-            import torch.distributed as tdist
-
-            tdist.destroy_process_group()
+    with Replicas("nccl", timeout_s=120) as rep:
+        run_ours(args, rep)
 
 
 if __name__ == "__main__":

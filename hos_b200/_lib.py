@@ -86,6 +86,8 @@ _SIGNATURES = {
     "hos_get_state_physical": (_I, [_H, _P, _P]),
     "hos_step": (_I, [_H, _D, _I]),
     "hos_sync": (_I, [_H]),
+    "hos_health": (_I, [_H, ctypes.POINTER(ctypes.c_longlong)]),
+    "hos_inject_alloc_failure": (None, [ctypes.c_long]),
     "hos_energy_history": (_I, [_H, _P, _P, _I, ctypes.POINTER(_I)]),
     "hos_clear_history": (_I, [_H]),
     "hos_rhs": (_I, [_H, _P, _P, _D]),
@@ -105,6 +107,7 @@ _SIGNATURES = {
     "hos_ensemble_step": (_I, [_H, _I]),
     "hos_ensemble_sync": (_I, [_H]),
     "hos_ensemble_info": (_I, [_H, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "hos_ensemble_stream": (_P, [_H]),
     "hos_ensemble_destroy": (_I, [_H]),
     "hos_last_error": (ctypes.c_char_p, []),
     "hos_version": (ctypes.c_char_p, []),

@@ -24,6 +24,7 @@
 #include <mutex>
 #include <string>
 #include <algorithm>
+#include <atomic>
 #include <map>
 #include <vector>
 
@@ -94,24 +95,27 @@ struct StepEndArgs {
   double* ham_hist;
   double* t_hist;
   int hist_cap;
+  long long* bad_step;  // first step whose energy was not finite (-1: none)
+  int* any_bad;         // ensemble-wide word set with bad_step (nullptr outside ensembles)
 };
 
 __device__ void step_end_body(const double* ham_part, int nparts, double* tdev, double dt, long long* stepdev,
-                              double* ham_hist, double* t_hist, int hist_cap);
+                              double* ham_hist, double* t_hist, int hist_cap, long long* bad_step, int* any_bad);
 
 __global__ void __launch_bounds__(256) k_step_end(const double* ham_part, int nparts, double* tdev, double dt,
-                                                  long long* stepdev, double* ham_hist, double* t_hist, int hist_cap) {
-  step_end_body(ham_part, nparts, tdev, dt, stepdev, ham_hist, t_hist, hist_cap);
+                                                  long long* stepdev, double* ham_hist, double* t_hist, int hist_cap,
+                                                  long long* bad_step) {
+  step_end_body(ham_part, nparts, tdev, dt, stepdev, ham_hist, t_hist, hist_cap, bad_step, nullptr);
 }
 
 // One block per ensemble member.
 __global__ void __launch_bounds__(256) k_step_end_b(const StepEndArgs* __restrict__ arr) {
   const StepEndArgs& a = arr[blockIdx.x];
-  step_end_body(a.ham_part, a.nparts, a.tdev, a.dt, a.stepdev, a.ham_hist, a.t_hist, a.hist_cap);
+  step_end_body(a.ham_part, a.nparts, a.tdev, a.dt, a.stepdev, a.ham_hist, a.t_hist, a.hist_cap, a.bad_step, a.any_bad);
 }
 
 __device__ void step_end_body(const double* ham_part, int nparts, double* tdev, double dt, long long* stepdev,
-                              double* ham_hist, double* t_hist, int hist_cap) {
+                              double* ham_hist, double* t_hist, int hist_cap, long long* bad_step, int* any_bad) {
   __shared__ double red[256];
   double s = 0.0;
   for (int i = threadIdx.x; i < nparts; i += blockDim.x) s += ham_part[i];
@@ -126,6 +130,12 @@ __device__ void step_end_body(const double* ham_part, int nparts, double* tdev, 
   if (st >= 0) {  // ring of hist_cap records
     ham_hist[st % hist_cap] = red[0];
     t_hist[st % hist_cap] = *tdev;
+  }
+  // the energy sums every mode of eta and phi, so a NaN or Inf anywhere in the
+  // state shows here; the host reads this word at hos_sync
+  if (!isfinite(red[0])) {
+    if (*bad_step < 0) *bad_step = st;
+    if (any_bad) *any_bad = 1;
   }
   *tdev = *tdev + dt;
   *stepdev = st + 1;
@@ -387,6 +397,7 @@ struct hos_ctx {
   double* trhs = nullptr;
   double* rdev = nullptr;
   long long* stepdev = nullptr;
+  long long* bad_step = nullptr;  // first step with a non-finite energy (-1: none)
   int* actdev = nullptr;
   int* flagdev = nullptr;
   double* ham_part = nullptr;
@@ -873,7 +884,7 @@ int enqueue_step(hos_ctx* c, double dt) {
     if (rc) return rc;
   }
   k_step_end<<<1, 256, 0, c->st>>>(c->ham_part, xgrid(c, c->cfg.xf), c->tdev, dt, c->stepdev, c->ham_hist, c->t_hist,
-                                  HIST_CAP);
+                                  HIST_CAP, c->bad_step);
   return HOS_OK;
 }
 
@@ -958,7 +969,7 @@ void release(hos_ctx* c) {
   if (!c) return;
   if (c->gexec) cudaGraphExecDestroy(c->gexec);
   if (c->graph) cudaGraphDestroy(c->graph);
-  void* ptrs[] = {c->u,    c->k,    c->zbuf,    c->phys,   c->ustage, c->ustg, c->zplain,   c->pplain,
+  void* ptrs[] = {c->bad_step, c->u,    c->k,    c->zbuf,    c->phys,   c->ustage, c->ustg, c->zplain,   c->pplain,
                   c->tdev, c->trhs, c->rdev,    c->stepdev, c->actdev, c->flagdev, c->ham_part,
                   c->ham_hist, c->t_hist, c->zvbuf, c->hpart, c->tw[0][0], c->tw[0][1], c->tw[0][2], c->tw[1][0], c->tw[1][1], c->tw[1][2]};
   for (void* p : ptrs)
@@ -967,8 +978,30 @@ void release(hos_ctx* c) {
   delete c;
 }
 
+// Fault injection for tests: after `limit` further device allocations, the
+// next ones fail as if the device were out of memory.  The limit comes from
+// HOS_FAIL_ALLOC_AFTER in the environment or from hos_inject_alloc_failure;
+// -1 (the default) disables it.
+std::atomic<long> g_alloc_count{0};
+std::atomic<long> g_alloc_limit{-2};  // -2: not yet read from the environment
+
+bool injected_alloc_failure() {
+  long lim = g_alloc_limit.load();
+  if (lim == -2) {
+    const char* s = getenv("HOS_FAIL_ALLOC_AFTER");
+    long expect = -2;
+    g_alloc_limit.compare_exchange_strong(expect, s ? atol(s) : -1L);
+    lim = g_alloc_limit.load();
+  }
+  return lim >= 0 && g_alloc_count.fetch_add(1) >= lim;
+}
+
 template <typename P>
 int dalloc(P** p, size_t bytes) {
+  if (injected_alloc_failure()) {
+    *p = nullptr;
+    return fail(HOS_ERR_NOMEM, "cudaMalloc(%zu): injected failure (HOS_FAIL_ALLOC_AFTER)", bytes);
+  }
   cudaError_t e = cudaMalloc((void**)p, bytes ? bytes : 16);
   if (e != cudaSuccess) {
     (void)cudaGetLastError();
@@ -1002,6 +1035,7 @@ struct hos_ens {
   cudaEvent_t fork = nullptr;
   void* dargs = nullptr;
   size_t dargs_bytes = 0;
+  int* any_bad = nullptr;  // set by a member's step end when its energy is not finite
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   int launches_per_step = 0;
@@ -1081,7 +1115,7 @@ int plan_step(hos_ens* E, std::vector<std::vector<BatchLaunch>>& per_class, std:
     for (int f : K.idx) {
       hos_ctx* c = E->mem[f];
       se.push_back(StepEndArgs{c->ham_part, xgrid(c, c->cfg.xf), c->tdev, E->dt[f], c->stepdev, c->ham_hist,
-                               c->t_hist, HIST_CAP});
+                               c->t_hist, HIST_CAP, c->bad_step, E->any_bad});
     }
     end_off.push_back(put(se.data(), se.size() * sizeof(StepEndArgs)));
     ends.insert(ends.end(), se.begin(), se.end());
@@ -1154,6 +1188,7 @@ void release_ens(hos_ens* E) {
   if (E->gexec) cudaGraphExecDestroy(E->gexec);
   if (E->graph) cudaGraphDestroy(E->graph);
   if (E->dargs) cudaFree(E->dargs);
+  if (E->any_bad) cudaFree(E->any_bad);
   for (EnsClass& K : E->cls) {
     if (K.join) cudaEventDestroy(K.join);
     if (K.st) cudaStreamDestroy(K.st);
@@ -1275,6 +1310,7 @@ int hos_create(const hos_params* p, hos_handle* out) {
   HOS_AL(c->trhs, sizeof(double));
   HOS_AL(c->rdev, sizeof(double));
   HOS_AL(c->stepdev, sizeof(long long));
+  HOS_AL(c->bad_step, sizeof(long long));
   HOS_AL(c->actdev, sizeof(int));
   HOS_AL(c->flagdev, sizeof(int));
   HOS_AL(c->ham_hist, HIST_CAP * sizeof(double));
@@ -1326,6 +1362,7 @@ int hos_create(const hos_params* p, hos_handle* out) {
   if (e == cudaSuccess) e = cudaMemsetAsync(c->tdev, 0, sizeof(double), c->st);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->trhs, 0, sizeof(double), c->st);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->stepdev, 0, sizeof(long long), c->st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->bad_step, 0xff, sizeof(long long), c->st);  // -1
   if (e == cudaSuccess) e = cudaMemsetAsync(c->ham_part, 0, (size_t)c->nparts * sizeof(double), c->st);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->ham_hist, 0, HIST_CAP * sizeof(double), c->st);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->t_hist, 0, HIST_CAP * sizeof(double), c->st);
@@ -1360,6 +1397,7 @@ void* hos_stream(hos_handle h) { return h ? (void*)h->st : nullptr; }
 
 int hos_set_state_spectral(hos_handle h, const double* u, double t) {
   if (!h || !u) return fail(HOS_ERR_ARG, "null argument");
+  HOS_CK(cudaMemsetAsync(h->bad_step, 0xff, sizeof(long long), h->st));
   HOS_CK(cudaMemcpyAsync(h->u, u, 2 * h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
   HOS_CK(cudaMemcpyAsync(h->tdev, &t, sizeof(double), cudaMemcpyHostToDevice, h->st));
   refresh_active_rows(h, h->u, h->actdev);
@@ -1380,6 +1418,7 @@ int hos_get_state_spectral(hos_handle h, double* u, double* t) {
 
 int hos_set_state_physical(hos_handle h, const double* eta, const double* phi, double t) {
   if (!h || !eta || !phi) return fail(HOS_ERR_ARG, "null argument");
+  HOS_CK(cudaMemsetAsync(h->bad_step, 0xff, sizeof(long long), h->st));
   HOS_CK(cudaMemcpyAsync(h->pplain, eta, h->psz * sizeof(double), cudaMemcpyDefault, h->st));
   HOS_CK(cudaMemcpyAsync(h->pplain + h->psz, phi, h->psz * sizeof(double), cudaMemcpyDefault, h->st));
   enqueue_r2c(h, h->pplain, h->u, 1);
@@ -1416,6 +1455,21 @@ int hos_sync(hos_handle h) {
   if (!h) return fail(HOS_ERR_ARG, "null handle");
   HOS_CK(cudaStreamSynchronize(h->st));
   HOS_CK(cudaGetLastError());
+  long long bad = -1;
+  HOS_CK(cudaMemcpy(&bad, h->bad_step, sizeof(long long), cudaMemcpyDeviceToHost));
+  if (bad >= 0) return fail(HOS_ERR_NONFINITE, "the state became non-finite at step %lld", bad);
+  return HOS_OK;
+}
+
+void hos_inject_alloc_failure(long after) {
+  g_alloc_count.store(0);
+  g_alloc_limit.store(after < 0 ? -1 : after);
+}
+
+int hos_health(hos_handle h, long long* first_nonfinite_step) {
+  if (!h || !first_nonfinite_step) return fail(HOS_ERR_ARG, "null argument");
+  HOS_CK(cudaStreamSynchronize(h->st));
+  HOS_CK(cudaMemcpy(first_nonfinite_step, h->bad_step, sizeof(long long), cudaMemcpyDeviceToHost));
   return HOS_OK;
 }
 
@@ -1680,7 +1734,13 @@ int hos_ensemble_create(const hos_handle* members, const double* dt, int n, hos_
       return fail(HOS_ERR_CUDA, "member sync: %s", cudaGetErrorString(err));
     }
   }
-  int rc = build_ens_graph(E);
+  int rc = dalloc(&E->any_bad, sizeof(int));
+  if (rc == HOS_OK && cudaMemset(E->any_bad, 0, sizeof(int)) != cudaSuccess) rc = fail(HOS_ERR_CUDA, "memset");
+  if (rc) {
+    release_ens(E);
+    return rc;
+  }
+  rc = build_ens_graph(E);
   if (rc) {
     release_ens(E);
     return rc;
@@ -1699,8 +1759,13 @@ int hos_ensemble_sync(hos_ensemble e) {
   if (!e) return fail(HOS_ERR_ARG, "null ensemble");
   HOS_CK(cudaStreamSynchronize(e->st));
   HOS_CK(cudaGetLastError());
+  int bad = 0;
+  HOS_CK(cudaMemcpy(&bad, e->any_bad, sizeof(int), cudaMemcpyDeviceToHost));
+  if (bad) return fail(HOS_ERR_NONFINITE, "a member's state became non-finite (hos_health on each member tells which)");
   return HOS_OK;
 }
+
+void* hos_ensemble_stream(hos_ensemble e) { return e ? (void*)e->st : nullptr; }
 
 int hos_ensemble_info(hos_ensemble e, int* nclasses, int* launches_per_step) {
   if (!e) return fail(HOS_ERR_ARG, "null ensemble");

@@ -35,6 +35,11 @@ class HosEnsemble:
         _lib.check(self._lib.hos_ensemble_sync(self._h))
 
     @property
+    def stream(self):
+        """cudaStream_t (as an int) the step graphs run on."""
+        return self._lib.hos_ensemble_stream(self._h)
+
+    @property
     def info(self):
         nc, nl = ctypes.c_int(), ctypes.c_int()
         _lib.check(self._lib.hos_ensemble_info(self._h, ctypes.byref(nc), ctypes.byref(nl)))

@@ -168,7 +168,15 @@ class HosField:
         _lib.check(self._lib.hos_step(self._h, float(dt), int(nsteps)))
 
     def sync(self):
+        """Waits for queued steps; raises HosError (code HOS_ERR_NONFINITE)
+        when a step's energy was NaN or Inf."""
         _lib.check(self._lib.hos_sync(self._h))
+
+    def health(self):
+        """First step whose energy was not finite, or None."""
+        s = ctypes.c_longlong()
+        _lib.check(self._lib.hos_health(self._h, ctypes.byref(s)))
+        return None if s.value < 0 else s.value
 
     def energy_history(self, max_records=1 << 16):
         t = np.zeros(max_records)

@@ -15,7 +15,10 @@ number of RK4 steps).  The server
   boundary, and finished ones leave (their slot and memory are freed);
 * records for each request its arrival, admission and completion times; the
   time-to-result is completion minus arrival and includes reading the
-  result (eta, phi) back to the host.
+  result (eta, phi) back to the host;
+* fails a request alone when its state becomes non-finite (the step-end
+  energy check on the device flags the member; the others continue), and
+  takes cancellations between chunks.
 
 Each field advances by exactly the same kernel sequence whether it runs
 alone or among others, so a result does not depend on the mix
@@ -28,11 +31,14 @@ does not hold the loop.
 from __future__ import annotations
 
 import math
+import threading
 import time
 from dataclasses import dataclass, field
 
 import numpy as np
 
+from ._lib import HOS_ERR_NONFINITE, HosError
+from ._lib import check as _lib_check
 from .ensemble import HosEnsemble
 from .field import HosField
 
@@ -52,6 +58,8 @@ class Request:
     # filled by the server
     admitted: float | None = None
     finished: float | None = None
+    status: str = "queued"  # queued, active, done, failed, cancelled, rejected
+    error: str | None = None
     result: tuple | None = field(default=None, repr=False)
 
     @property
@@ -103,101 +111,235 @@ def jonswap_device(n, kp, steepness, seed, depth=None, gamma=3.3, spread_s=10.0,
     return (eta * scale).contiguous(), (phi * scale).contiguous(), 2 * math.pi / wp
 
 
+class DeviceBackend:
+    """The server's device side: one ``HosField`` per admitted request, one
+    ``HosEnsemble`` over the active fields.  The request loop in ``Server``
+    only calls these methods, so that its queueing, admission, cancellation
+    and failure handling can be exercised without a GPU."""
+
+    def footprint(self, r):
+        return HosField.footprint_bytes(r.n, r.n, r.order, r.precision)
+
+    def free_bytes(self):
+        import torch
+
+        return torch.cuda.mem_get_info()[0]
+
+    def open(self, r):
+        """Creates the request's field with its initial sea; returns (field, dt)."""
+        eta, phi, tp = jonswap_device(r.n, r.kp_value, r.steepness, r.seed, depth=r.depth)
+        f = HosField(r.n, r.n, order=r.order, precision=r.precision, depth=r.depth)
+        try:
+            _lib_check(f._lib.hos_set_state_physical(f._h, _dptr(eta), _dptr(phi), 0.0))
+        except Exception:
+            f.close()
+            raise
+        return f, tp / 50
+
+    def group(self, fields, dts):
+        return HosEnsemble(fields, dts)
+
+    def advance(self, group, steps):
+        """Advances every member; returns False when some member's state
+        became non-finite (the others are unaffected)."""
+        group.step(steps)
+        try:
+            group.sync()
+        except HosError as e:
+            if e.code != HOS_ERR_NONFINITE:
+                raise
+            return False
+        return True
+
+    def failed_step(self, f):
+        return f.health()
+
+    def result(self, f):
+        return f.state_physical()
+
+    def close(self, obj):
+        obj.close()
+
+
 class Server:
-    def __init__(self, chunk=25, max_slots=4096, reserve_bytes=2 << 30, hbm_budget_bytes=None, keep_results=True):
+    """Continuous-batching request loop (see the module docstring).
+
+    ``run(requests)`` serves a list and returns metrics; ``submit`` and
+    ``cancel`` may be called from other threads while ``run`` is active (a
+    cancelled request leaves at the next chunk boundary, or before admission
+    if it is still queued).  With ``wait_for_more=True`` the loop idles for
+    new submissions until ``stop()`` is called.
+
+    Each request ends with ``status``: "done" (result read back), "failed"
+    (its state became non-finite; ``error`` says at which step; the other
+    fields of the batch continue unaffected), "cancelled", or "rejected" (its
+    footprint exceeds what the device offers with the server holding
+    nothing)."""
+
+    def __init__(self, chunk=25, max_slots=4096, reserve_bytes=2 << 30, hbm_budget_bytes=None, keep_results=True,
+                 backend=None):
         self.chunk = int(chunk)
         self.max_slots = int(max_slots)
         self.reserve = int(reserve_bytes)
         self.budget = hbm_budget_bytes  # optional cap on what the server may hold
         self.keep_results = keep_results
+        self.backend = backend if backend is not None else DeviceBackend()
         self.rebuilds = 0
         self.chunks = 0
+        self._mu = threading.Lock()
+        self._incoming = []
+        self._cancelled = set()
+        self._stop = threading.Event()
 
-    def _free_bytes(self, held):
-        import torch
+    # ------------------------------------------------------------ other threads
+    def submit(self, req):
+        """Queues a request; its ``arrival`` is taken as seconds after the
+        start of the current (or next) ``run``."""
+        with self._mu:
+            self._incoming.append(req)
 
-        free, _total = torch.cuda.mem_get_info()
-        avail = free - self.reserve
+    def cancel(self, rid):
+        with self._mu:
+            self._cancelled.add(rid)
+
+    def stop(self):
+        self._stop.set()
+
+    # ------------------------------------------------------------ the loop
+    def _avail(self, held):
+        avail = self.backend.free_bytes() - self.reserve
         if self.budget is not None:
             avail = min(avail, self.budget - held)
         return avail
 
-    def run(self, requests, realtime=True, time_limit=None):
-        """Serve the requests (sorted by arrival).  With realtime, a request
-        becomes visible at its arrival time on the wall clock; otherwise all
-        are visible at once.  Returns a metrics dict."""
+    def run(self, requests=(), realtime=True, time_limit=None, wait_for_more=False):
+        """Serve the requests (sorted by arrival) and any submitted meanwhile.
+        With realtime, a request becomes visible at its arrival time on the
+        wall clock; otherwise all are visible at once.  Returns a metrics
+        dict."""
+        be = self.backend
+        self._stop.clear()
         pending = sorted(requests, key=lambda r: r.arrival)
+        submitted = len(pending)
         active = []  # [req, field, dt, remaining]
         done = []
+        ended = []  # failed, cancelled and rejected requests
         held = 0
         ens = None
         dirty = False
         gp_steps = 0.0
         t0 = time.perf_counter()
-        while pending or active:
+
+        def retire(a, status, error=None):
+            nonlocal held
+            r = a[0]
+            r.status, r.error = status, error
+            r.finished = time.perf_counter() - t0
+            be.close(a[1])
+            held -= be.footprint(r)
+            ended.append(r)
+
+        while True:
+            with self._mu:
+                if self._incoming:
+                    submitted += len(self._incoming)
+                    pending = sorted(pending + self._incoming, key=lambda r: r.arrival)
+                    self._incoming = []
+                cancelled = set(self._cancelled)
+            if not (pending or active):
+                if wait_for_more and not self._stop.is_set():
+                    time.sleep(0.002)
+                    continue
+                break
             now = time.perf_counter() - t0
             if time_limit is not None and now > time_limit:
                 break
-            # admission
+            # cancellation: queued requests leave at once, active ones here,
+            # at a chunk boundary
+            for r in [r for r in pending if r.rid in cancelled]:
+                r.status = "cancelled"
+                pending.remove(r)
+                ended.append(r)
+            gone = [a for a in active if a[0].rid in cancelled]
+            for a in gone:
+                retire(a, "cancelled")
+            if gone:
+                active = [a for a in active if a[0].rid not in cancelled]
+                dirty = True
+            # admission, in arrival order; a request that does not fit does
+            # not block smaller ones behind it
             visible = [r for r in pending if (not realtime) or r.arrival <= now]
             for r in visible:
                 if len(active) >= self.max_slots:
                     break
-                need = HosField.footprint_bytes(r.n, r.n, r.order, r.precision)
-                if need > self._free_bytes(held):
+                need = be.footprint(r)
+                if need > self._avail(held):
+                    if not active and held == 0:
+                        r.status, r.error = "rejected", f"needs {need} bytes of device memory"
+                        pending.remove(r)
+                        ended.append(r)
                     continue
-                eta, phi, tp = jonswap_device(r.n, r.kp_value, r.steepness, r.seed, depth=r.depth)
-                f = HosField(r.n, r.n, order=r.order, precision=r.precision, depth=r.depth)
-                f._lib.hos_set_state_physical(f._h, _dptr(eta), _dptr(phi), 0.0)
+                f, dt = be.open(r)
                 r.admitted = time.perf_counter() - t0
-                active.append([r, f, tp / 50, r.steps])
+                r.status = "active"
+                active.append([r, f, dt, r.steps])
                 held += need
                 pending.remove(r)
                 dirty = True
             if not active:
                 if pending and realtime:
                     time.sleep(max(0.0, min(0.002, pending[0].arrival - now)))
-                elif pending:
-                    raise RuntimeError("a request does not fit in device memory even alone")
                 continue
             if dirty:
                 if ens is not None:
-                    ens.close()
-                ens = HosEnsemble([a[1] for a in active], [a[2] for a in active])
+                    be.close(ens)
+                ens = be.group([a[1] for a in active], [a[2] for a in active])
                 self.rebuilds += 1
                 dirty = False
             steps = min(self.chunk, min(a[3] for a in active))
-            ens.step(steps)
-            ens.sync()
+            healthy = be.advance(ens, steps)
             self.chunks += 1
+            if not healthy:
+                bad = [(a, be.failed_step(a[1])) for a in active]
+                bad = [(a, s) for a, s in bad if s is not None]
+                for a, s in bad:
+                    retire(a, "failed", f"state became non-finite at step {s}")
+                ids = {id(a) for a, _ in bad}
+                active = [a for a in active if id(a) not in ids]
+                dirty = True
             for a in active:
                 a[3] -= steps
                 gp_steps += steps * a[0].n * a[0].n
             finished = [a for a in active if a[3] == 0]
+            for a in finished:
+                r, f = a[0], a[1]
+                res = be.result(f)
+                r.finished = time.perf_counter() - t0
+                r.status = "done"
+                if self.keep_results:
+                    r.result = res
+                be.close(f)
+                held -= be.footprint(r)
+                done.append(r)
             if finished:
-                for a in finished:
-                    r, f = a[0], a[1]
-                    eta, phi = f.state_physical()
-                    r.finished = time.perf_counter() - t0
-                    if self.keep_results:
-                        r.result = (eta, phi)
-                    f.close()
-                    held -= HosField.footprint_bytes(r.n, r.n, r.order, r.precision)
-                    done.append(r)
                 active = [a for a in active if a[3] > 0]
-                if ens is not None:
-                    ens.close()
-                    ens = None
-                dirty = bool(active)
+                dirty = True
+            if dirty and ens is not None:
+                be.close(ens)
+                ens = None
         if ens is not None:
-            ens.close()
+            be.close(ens)
         for a in active:
-            a[1].close()
+            be.close(a[1])
         wall = time.perf_counter() - t0
         ttr = np.array([r.finished - r.arrival for r in done]) if done else np.zeros(0)
+        count = lambda st: sum(1 for r in ended if r.status == st)  # noqa: E731
         return {
             "completed": len(done),
-            "submitted": len(requests),
+            "submitted": submitted,
+            "failed": count("failed"),
+            "cancelled": count("cancelled"),
+            "rejected": count("rejected"),
             "wall_s": wall,
             "p50_s": float(np.percentile(ttr, 50)) if len(ttr) else None,
             "p99_s": float(np.percentile(ttr, 99)) if len(ttr) else None,

@@ -103,7 +103,18 @@ int hos_get_state_physical(hos_handle h, double* eta, double* phi);
  * time_schemes_par.c:28-121, called nsteps times).  Asynchronous with
  * respect to the host; hos_sync waits. */
 int hos_step(hos_handle h, double dt, int nsteps);
+/* Waits for the handle's work.  Returns HOS_ERR_NONFINITE when a step's
+ * energy was NaN or Inf, i.e. the state became non-finite (set on the device
+ * by the step-end reduction; cleared by the next hos_set_state_*). */
 int hos_sync(hos_handle h);
+/* First step whose energy was not finite, or -1 (steps are counted from
+ * hos_create: 0 is the handle's first step). */
+int hos_health(hos_handle h, long long* first_nonfinite_step);
+/* Test hook: the device allocations after the next `after` ones fail with
+ * HOS_ERR_NOMEM (the call that hits it frees what it had allocated);
+ * after < 0 turns it off.  HOS_FAIL_ALLOC_AFTER in the environment sets the
+ * initial value. */
+void hos_inject_alloc_failure(long after);
 
 /* Stage-0 Hamiltonian of each step (hosm_2d_par.c:462-523, logged by the
  * reference to runtime.dat at time_schemes_par.c:73-93) and the step-start
@@ -172,6 +183,8 @@ int hos_ensemble_create(const hos_handle* members, const double* dt, int n, hos_
 int hos_ensemble_step(hos_ensemble e, int nsteps);
 int hos_ensemble_sync(hos_ensemble e);
 int hos_ensemble_info(hos_ensemble e, int* nclasses, int* launches_per_step);
+/* The stream the ensemble's step graphs are launched on (cudaStream_t). */
+void* hos_ensemble_stream(hos_ensemble e);
 int hos_ensemble_destroy(hos_ensemble e);
 
 /* Kernel launches of this library in one RK step of the handle. */
