@@ -207,6 +207,30 @@ int hos_launches_per_step(hos_handle h);
  * order them on one stream. */
 int hos_fft_2d_noalloc(const double* u_phys, double* hu, int nx, int ny, void* stream);
 
+/* ------------------------------------------------------------------ HDF5 files
+ * The subset of the HDF5 format the driver's files use, without libhdf5:
+ * superblock v0/v1, root-group datasets with version 1 object headers,
+ * contiguous or compact storage.  Replaces get_params / get_ic_2d
+ * (hdf5_routines_2d_par.c:13-101, :104-188), which read every dataset as
+ * H5T_IEEE_F64LE whatever its stored type (integers and floats convert), and
+ * the snapshot writers (write_header_2d :227-283, write_field_2d :286-392,
+ * write_coordinates_2d :395-446, write_extra_2d :449-537), which write 1x1
+ * header datasets and [Nx][Ny] fields into a new file.  Errors (missing file
+ * or dataset, unsupported storage, size mismatch) return HOS_ERR_ARG with
+ * the reason in hos_last_error(). */
+enum { HOS_H5_F64 = 0, HOS_H5_F32 = 1, HOS_H5_I64 = 2, HOS_H5_I32 = 3 };
+/* Names of the root group's datasets, one per line, into names[cap]. */
+int hos_h5_list(const char* path, char* names, int cap, int* count);
+/* Rank, dimensions (up to 4) and stored type (HOS_H5_*, -1 for other sizes). */
+int hos_h5_info(const char* path, const char* name, int* rank, long long* dims, int* type);
+/* Reads all nelems elements (row-major) as doubles. */
+int hos_h5_read_f64(const char* path, const char* name, double* out, long long nelems);
+/* Writes a new file (replacing any) holding n datasets of rank 0..2:
+ * dims[2*i..2*i+1] are dataset i's dimensions, data[i] its little-endian
+ * elements of type types[i] (HOS_H5_F64, HOS_H5_F32 or HOS_H5_I64). */
+int hos_h5_write(const char* path, int n, const char* const* names, const void* const* data, const int* types,
+                 const int* ranks, const long long* dims);
+
 /* CUDA stream of the handle (a cudaStream_t), for callers that order their
  * own work against it. */
 void* hos_stream(hos_handle h);

@@ -9,7 +9,9 @@ Run from the repository root after `make -C oracle`:
 
 Every case stores its inputs and the oracle's outputs in one .npz file.  The
 reference ships no test vectors of its own, so these fixtures are the
-pinned record of what the reference code computes on seeded inputs.
+pinned record of what the reference code computes on seeded inputs and on
+the one input file the reference ships (`python tests/golden/make_golden.py
+shipped` makes that case alone).
 """
 from __future__ import annotations
 
@@ -109,6 +111,36 @@ def main():
     save("jonswap64_m5_ramp_20", eta0=eta, phi0=phi, u0=u0, u20=u20, t20=t20, ham=ham, dt=0.2,
          meta=np.array([nx, ny, 5, 2]), lx=L, g=9.81, tramp=200.0)
 
+    shipped_case()
+
+
+def shipped_case():
+    """The reference's shipped input (Csource/2dpar/initpars.h5 and
+    initdata.1.h5, 256^2 JONSWAP, read with the library's HDF5 subset) run as
+    the reference's driver runs it: M = 3 (NLevs = 2), scheme 4 (midpoint),
+    dt = 0.2, ramp on with Tramp = 200, to T = 50 (250 steps).  Stored: the
+    dealiased initial spectrum and the final one as (row, column, value) over
+    the modes the dealias mask keeps, and the energy series."""
+    from hos_b200 import h5
+
+    src = "/root/reference/Csource/2dpar"
+    p = h5.read_params(os.path.join(src, "initpars.h5"))
+    eta = h5.read(os.path.join(src, "initdata.1.h5"), "eta0")
+    phi = h5.read(os.path.join(src, "initdata.1.h5"), "phi0")
+    nx, ny = p["Nx"], p["Ny"]
+    ref = RefC(3, nx, ny, lx=p["Lx"], ly=p["Ly"], g=p["g"], rampflg=p["rampflg"], tramp=p["Tramp"], scheme=4)
+    u0 = ref.init_state(eta, phi)
+    nsteps = int(round(p["T"] / 0.2))
+    u1, t1, ham = ref.steps(u0, 0.0, 0.2, nsteps)
+    keep = np.nonzero(HosNumpy(nx, ny, p["Lx"], p["Ly"], p["g"], 3).Dealias(np.ones((ny // 2 + 1, nx))))
+    save("shipped256_m3_mid_250", rows=keep[0].astype(np.int16), cols=keep[1].astype(np.int16),
+         u0=u0[:, keep[0], keep[1]], u250=u1[:, keep[0], keep[1]], t250=t1, ham=ham, dt=0.2,
+         meta=np.array([nx, ny, 3, 4, p["rampflg"]]), lx=p["Lx"], ly=p["Ly"], g=p["g"], tramp=p["Tramp"],
+         eta_l2=np.linalg.norm(eta), eta_sum=eta.sum())
+
 
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1 and sys.argv[1] == "shipped":
+        shipped_case()
+    else:
+        main()
