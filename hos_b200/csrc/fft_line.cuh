@@ -302,12 +302,25 @@ __device__ __forceinline__ void line_fft(cpx<T> (&v)[E], cpx<T>* sm, int t, cons
     if (!last) {
       constexpr int Q = 128 / (int)sizeof(C);
       line_sync<P>();
+      // The swizzled slots are formed from one swizzled base per thread:
+      // base has no bits where r*ns lies and the swizzle term never reads
+      // those bits, so slot(base + r*ns) = slot(base) ^ r*ns; for the reads
+      // (Q <= P) the term of e*P is a per-e constant below bit log2(P), so
+      // slot(t + e*P) = (slot(t) ^ const_e) + e*P, an immediate offset.
       const int base = (t / ns) * ns * E + (t & (ns - 1));
+      const int w0 = sswz<E, Q>(base, ns);
 #pragma unroll
-      for (int r = 0; r < E; r++) sm[sswz<E, Q>(base + r * ns, ns)] = v[r];
+      for (int r = 0; r < E; r++) sm[w0 ^ (r * ns)] = v[r];
       line_sync<P>();
+      if (Q <= P) {
+        const int r0 = sswz<E, Q>(t, ns);
+        const int mask = ns >= Q ? 0 : ((Q / ns) - 1) * ns;
 #pragma unroll
-      for (int e = 0; e < E; e++) v[e] = sm[sswz<E, Q>(t + e * P, ns)];
+        for (int e = 0; e < E; e++) v[e] = sm[(r0 ^ (((e * P) >> LP::LOGE) & mask)) + e * P];
+      } else {
+#pragma unroll
+        for (int e = 0; e < E; e++) v[e] = sm[sswz<E, Q>(t + e * P, ns)];
+      }
     }
     ns *= E;
   }

@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <atomic>
 #include <map>
+#include <utility>
 #include <vector>
 
 #include "hos_gpu.h"
@@ -116,6 +117,7 @@ __global__ void __launch_bounds__(256) k_step_end_b(const StepEndArgs* __restric
 
 __device__ void step_end_body(const double* ham_part, int nparts, double* tdev, double dt, long long* stepdev,
                               double* ham_hist, double* t_hist, int hist_cap, long long* bad_step, int* any_bad) {
+  pdl_enter();
   __shared__ double red[256];
   double s = 0.0;
   for (int i = threadIdx.x; i < nparts; i += blockDim.x) s += ham_part[i];
@@ -854,15 +856,50 @@ void build_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, doub
   out.push_back(r7);
 }
 
+// Programmatic dependent launch of the passes of one field (the kernels
+// wait for their predecessor at entry, see pdl_enter): the next pass is
+// launched and its blocks placed while the previous one drains, which hides
+// the launch gap between the dependent passes of a step.  HOS_PDL=0 in the
+// environment launches them with plain stream order instead.
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* s = getenv("HOS_PDL");
+    return !(s && s[0] == '0');
+  }();
+  return on;
+}
+
+template <typename... K, typename... A>
+void launch_pdl(void (*kernel)(K...), dim3 grid, unsigned threads, size_t smem, cudaStream_t st, A&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  (void)cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);  // errors surface at the next check
+}
+
 // Launches one pass of one field with its arguments by value.
 void launch_single(hos_ctx* c, const PassRec& r) {
   const PassCfg& g = c->cfg;
   const dim3 grid(r.gx, r.gy);
+  const XInvArgs* nxi = nullptr;
+  const XFwdArgs* nxf = nullptr;
+  const YInvArgs* nyi = nullptr;
+  const YFwdArgs* nyf = nullptr;
+  const void* twx = g.twx;
+  const void* twh = g.twh;
+  const void* twy = g.twy;
   switch (r.kind) {
-    case L_XINV: g.xinv[r.mode]<<<grid, g.xi.threads, g.xi.smem, c->st>>>(r.xi, nullptr, g.twx); break;
-    case L_XFWD: g.xfwd[r.mode]<<<grid, g.xf.threads, g.xf.smem, c->st>>>(r.xf, nullptr, g.twx); break;
-    case L_YINV: g.yinv[r.mode]<<<grid, g.yi.threads, g.yi.smem, c->st>>>(r.yi, nullptr, g.twh, g.twy); break;
-    default: g.yfwd[r.mode]<<<grid, g.yf.threads, g.yf.smem, c->st>>>(r.yf, nullptr, g.twh, g.twy); break;
+    case L_XINV: launch_pdl(g.xinv[r.mode], grid, g.xi.threads, g.xi.smem, c->st, r.xi, nxi, twx); break;
+    case L_XFWD: launch_pdl(g.xfwd[r.mode], grid, g.xf.threads, g.xf.smem, c->st, r.xf, nxf, twx); break;
+    case L_YINV: launch_pdl(g.yinv[r.mode], grid, g.yi.threads, g.yi.smem, c->st, r.yi, nyi, twh, twy); break;
+    default: launch_pdl(g.yfwd[r.mode], grid, g.yf.threads, g.yf.smem, c->st, r.yf, nyf, twh, twy); break;
   }
 }
 
@@ -883,8 +920,9 @@ int enqueue_step(hos_ctx* c, double dt) {
     int rc = enqueue_stage(c, s, dt, false, c->u, c->k + (size_t)s * 2 * c->fsz, c->tdev, c->actdev);
     if (rc) return rc;
   }
-  k_step_end<<<1, 256, 0, c->st>>>(c->ham_part, xgrid(c, c->cfg.xf), c->tdev, dt, c->stepdev, c->ham_hist, c->t_hist,
-                                  HIST_CAP, c->bad_step);
+  const double* hp = c->ham_part;
+  launch_pdl(k_step_end, dim3(1), 256, 0, c->st, hp, xgrid(c, c->cfg.xf), c->tdev, dt, c->stepdev, c->ham_hist,
+             c->t_hist, (int)HIST_CAP, c->bad_step);
   return HOS_OK;
 }
 

@@ -82,6 +82,17 @@ __device__ __forceinline__ float dz_mult_t<float>(const Geo& G, int i, int j, in
   return m;
 }
 
+// Programmatic dependent launch.  The engine launches the passes of a step
+// with programmatic stream serialisation, so a pass can be launched and its
+// blocks placed while the previous pass drains.  Every such kernel first
+// waits for the previous grid to complete and its writes to be visible
+// (before it reads or writes global memory), then allows the next pass to
+// launch.  Launched without the attribute both instructions return at once.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
 enum { XI_STAGE = 0, XI_PLAIN = 1 };
 enum { XF_PLAIN = 0, XF_LEVEL = 1, XF_RHS = 2 };
 enum { YI_JOBS = 0, YI_LEVEL = 1 };
@@ -112,6 +123,7 @@ struct XInvArgs {
 template <typename T, int NX, int E, int MODE, bool B>
 __global__ void __launch_bounds__(MAX_THREADS, 2) k_xinv(const __grid_constant__ XInvArgs a0,
                                                          const XInvArgs* __restrict__ arr, const void* twv) {
+  pdl_enter();
   const XInvArgs& a = B ? arr[blockIdx.z] : a0;  // batched: one field per z
   if (B && (int)blockIdx.y >= a.ycount) return;
   using C = cpx<T>;
@@ -213,6 +225,7 @@ struct XFwdArgs {
 template <typename T, int NX, int E, int MODE, bool B>
 __global__ void __launch_bounds__(MAX_THREADS, 2) k_xfwd(const __grid_constant__ XFwdArgs a0,
                                                          const XFwdArgs* __restrict__ arr, const void* twv) {
+  pdl_enter();
   const XFwdArgs& a = B ? arr[blockIdx.z] : a0;
   if (B && (int)blockIdx.y >= a.ycount) return;
   using C = cpx<T>;
@@ -397,11 +410,27 @@ __device__ __forceinline__ void yfwd_finish(cpx<T> (&v)[E], cpx<T>* sm, cpx<T>* 
   }
   __syncthreads();
   const int ntot = G * rows_out;
+  const int lg = __ffs(G) - 1;  // G is a power of two
   for (int q = threadIdx.x; q < ntot; q += blockDim.x) {
-    const int ky = q / G, g = q - ky * G;
+    const int ky = q >> lg, g = q & (G - 1);
     vo[(size_t)ky * nx + ix0 + g] = sm[(size_t)g * lp + (ky)];
   }
 }
+
+// Asynchronous global -> shared copy of one complex element (cp.async, 8 or
+// 16 bytes); when `live` is false the shared element is zero-filled and the
+// source is not read.  cp_async_wait_all waits for this thread's copies;
+// a block barrier then makes all of them visible.
+template <typename C>
+__device__ __forceinline__ void cp_async_elem(C* dst, const C* src, bool live) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  const int n = live ? (int)sizeof(C) : 0;
+  if (sizeof(C) == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // ---------------------------------------------------------------- y passes
 // Shared memory of a y-pass block: G line regions of `lp` complex elements.
@@ -445,6 +474,7 @@ template <typename T, int H, int E, int MODE, bool B>
 __global__ void __launch_bounds__(MAX_THREADS, 2) k_yinv(const __grid_constant__ YInvArgs a0,
                                                          const YInvArgs* __restrict__ arr, const void* twv,
                                                          const void* twyv) {
+  pdl_enter();
   const YInvArgs& a = B ? arr[blockIdx.z] : a0;
   if (B && (int)blockIdx.y >= a.ycount) return;
   using C = cpx<T>;
@@ -467,14 +497,17 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yinv(const __grid_constant__
   const YJob J = a.jobs[blockIdx.y];
   T* pall = reinterpret_cast<T*>(a.phys);
 
-  {  // column strip -> line regions
+  {  // column strip -> line regions; every row's copy is in flight at once
     const C* zs = reinterpret_cast<const C*>(a.z) + (size_t)J.zin * fsz;
     const int nin = G * (a.rows_dev ? *a.rows_dev : a.rows_in);
     const int ntot = G * (H + 1);
+    const int lg = __ffs(G) - 1;  // G is a power of two
     for (int q = threadIdx.x; q < ntot; q += blockDim.x) {
-      const int ky = q / G, g = q - ky * G;
-      sm[(size_t)g * a.lp + (ky)] = (q < nin) ? zs[(size_t)ky * nx + ix0 + g] : mkc((T)0, (T)0);
+      const int ky = q >> lg, g = q & (G - 1);
+      const bool live = q < nin;
+      cp_async_elem(&sm[(size_t)g * a.lp + ky], live ? zs + (size_t)ky * nx + ix0 + g : zs, live);
     }
+    cp_async_wait_all();
   }
   __syncthreads();
   // complex-to-real preprocessing: c[k] = Xe + i Xo (packing of a length-Ny
@@ -623,6 +656,7 @@ template <typename T, int H, int E, int MODE, bool B>
 __global__ void __launch_bounds__(MAX_THREADS, 2) k_yfwd(const __grid_constant__ YFwdArgs a0,
                                                          const YFwdArgs* __restrict__ arr, const void* twv,
                                                          const void* twyv) {
+  pdl_enter();
   const YFwdArgs& a = B ? arr[blockIdx.z] : a0;
   if (B && (int)blockIdx.y >= a.ycount) return;
   using C = cpx<T>;
