@@ -205,6 +205,12 @@ __device__ __forceinline__ void dft(C* a) {
   for (int i = 0; i < R; i++) a[i] = b[i];
 }
 
+__host__ __device__ constexpr int hibit(int r) {
+  int h = 1;
+  while (h * 2 <= r) h *= 2;
+  return h;
+}
+
 template <int N>
 __device__ __forceinline__ constexpr int ilog2c() {
   int r = 0;
@@ -280,22 +286,18 @@ __device__ __forceinline__ void line_fft(cpx<T> (&v)[E], cpx<T>* sm, int t, cons
       // twiddle is at most log2(E)-1 products away from a table value
       const int jm = t & (ns - 1);
       const int scale = N / (ns * E);
-      C wp[LP::LOGE];
+      // w^r = w^(r - hi) * w^hi with hi the highest power of two in r: one
+      // product per non-power r, at most log2(E)-1 products deep
+      C wp[E];
 #pragma unroll
-      for (int b = 0; b < LP::LOGE; b++) wp[b] = twid<INV>(tw, (1 << b) * jm, scale);
+      for (int b = 0; b < LP::LOGE; b++) wp[1 << b] = twid<INV>(tw, (1 << b) * jm, scale);
 #pragma unroll
-      for (int r = 1; r < E; r++) {
-        C w;
-        bool first = true;
-#pragma unroll
-        for (int b = 0; b < LP::LOGE; b++) {
-          if (r & (1 << b)) {
-            w = first ? wp[b] : cmul(w, wp[b]);
-            first = false;
-          }
-        }
-        v[r] = cmul(v[r], w);
+      for (int r = 3; r < E; r++) {
+        const int hi = hibit(r);
+        if (r != hi) wp[r] = cmul(wp[r - hi], wp[hi]);
       }
+#pragma unroll
+      for (int r = 1; r < E; r++) v[r] = cmul(v[r], wp[r]);
     }
     dft<E, INV>(v);
     const bool last = (s == SF - 1) && (RL == 1);

@@ -72,9 +72,27 @@ __device__ __forceinline__ double dz_mult_t<double>(const Geo& G, int i, int j, 
   const double kx = kx_of(G, i), ky = ky_of(G, j);
   return dz_mult(G, sqrt(kx * kx + ky * ky), p);
 }
+// Wavenumbers in the compute precision T (single precision: formed from the
+// integer mode index and the single-precision 2 pi / L, no double arithmetic).
+template <typename T>
+__device__ __forceinline__ T kx_t(const Geo& G, int i) {
+  return (T)kx_of(G, i);
+}
+template <>
+__device__ __forceinline__ float kx_t<float>(const Geo& G, int i) {
+  return (float)(i <= G.nx / 2 + 1 ? i : i - G.nx) * (float)G.kx0;
+}
+template <typename T>
+__device__ __forceinline__ T ky_t(const Geo& G, int j) {
+  return (T)ky_of(G, j);
+}
+template <>
+__device__ __forceinline__ float ky_t<float>(const Geo& G, int j) {
+  return (float)j * (float)G.ky0;
+}
 template <>
 __device__ __forceinline__ float dz_mult_t<float>(const Geo& G, int i, int j, int p) {
-  const float kx = (float)kx_of(G, i), ky = (float)ky_of(G, j);
+  const float kx = kx_t<float>(G, i), ky = ky_t<float>(G, j);
   const float kz = sqrtf(kx * kx + ky * ky);
   float m = 1.0f;
   for (int q = 0; q < p; q++) m *= kz;
@@ -174,9 +192,9 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_xinv(const __grid_constant__
       }
       if ((o == 0 || o == 2) && live) a.ustg[foff + roff + i] = x;
       if (o == 1 || o == 3) {  // Dx: i kx (operators_par.c:66)
-        const double kx = kx_of(geo, i);
-        x = make_double2(-kx * x.y, kx * x.x);
-        v[e] = conv<T>(x);
+        const T kx = kx_t<T>(geo, i);
+        const C xc = conv<T>(x);
+        v[e] = mkc(-kx * xc.y, kx * xc.x);
       } else if (o >= 4) {  // Dz applied o-3 times (operators_par.c:168-192)
         v[e] = cscale(conv<T>(x), dz_mult_t<T>(geo, i, row, o - 3));
       } else {
@@ -519,7 +537,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yinv(const __grid_constant__
     C A = tl[(k)];
     C Bv = tl[(H - k)];
     if (J.iky) {
-      const T ka = (T)ky_of(geo, k), kb = (T)ky_of(geo, H - k);
+      const T ka = ky_t<T>(geo, k), kb = ky_t<T>(geo, H - k);
       A = cscale(cmul_i(A), ka);
       Bv = cscale(cmul_i(Bv), kb);
     }
