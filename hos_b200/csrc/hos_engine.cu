@@ -251,7 +251,7 @@ namespace {
 struct ElemChoice {
   int xi = 8, xf = 8, yi = 8, yf = 8;          // elements per thread
   int sxi = 0, sxf = 0, syi = 0, syf = 0;      // lines per block scaled by 2^s
-  int opb = 1;                                 // z-derivative orders per block of the level x-forward pass
+  int opb = 16;                                // z-derivative orders per block of the level x-forward pass (all)
   int fuse = 1;                                // next level's y-forward inside each level's y-inverse
 };
 
@@ -483,8 +483,15 @@ int pick_elems(int prec, int n, int want) {
 // Defaults: E = 8 for every pass kind measured fastest on B200 at 1024^2 in
 // both precisions; overridable through HOS_ELEMS="xi,xf,yi,yf".
 ElemChoice default_elems(int prec) {
-  (void)prec;
   ElemChoice ec;
+  // lines-per-block scales measured fastest on B200 at 1024^2, M = 5
+  if (prec) {
+    ec.sxi = 1;
+  } else {
+    ec.sxi = -1;
+    ec.syi = -1;
+    ec.syf = -1;
+  }
   if (const char* s = getenv("HOS_ELEMS")) {
     int a[4];
     if (sscanf(s, "%d,%d,%d,%d", &a[0], &a[1], &a[2], &a[3]) == 4) {
@@ -1364,10 +1371,14 @@ int hos_create(const hos_params* p, hos_handle* out) {
     if (p->tune[2]) ec.yi = p->tune[2];
     if (p->tune[3]) ec.yf = p->tune[3];
     auto clamp3 = [](int v) { return v < -3 ? -3 : (v > 3 ? 3 : v); };
-    ec.sxi = clamp3(p->tune[4]);
-    ec.sxf = clamp3(p->tune[5]);
-    ec.syi = clamp3(p->tune[6]);
-    ec.syf = clamp3(p->tune[7]);
+    bool tuned = false;
+    for (int i = 0; i < 8; i++) tuned = tuned || p->tune[i] != 0;
+    if (tuned) {  // a tuned shape sets every scale (0 included)
+      ec.sxi = clamp3(p->tune[4]);
+      ec.sxf = clamp3(p->tune[5]);
+      ec.syi = clamp3(p->tune[6]);
+      ec.syf = clamp3(p->tune[7]);
+    }
     if (p->tune_opb > 0) ec.opb = p->tune_opb;
     if (p->tune_nofuse) ec.fuse = 0;
     rc = make_cfg(c, c->prec, ec, &c->cfg);

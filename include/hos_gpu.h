@@ -66,7 +66,7 @@ typedef struct hos_params {
   int tune[8];      /* kernel shapes (0 = default): elements per thread of the x-inverse, x-forward,
                        y-inverse and y-forward passes (8, 16, or 32 in FP32), then the base-2 exponents
                        scaling their lines per block; chosen by hos_b200.autotune */
-  int tune_opb;     /* z-derivative orders per block of the level x-forward pass (0 = 1) */
+  int tune_opb;     /* z-derivative orders per block of the level x-forward pass (0 = all in one block) */
   int tune_nofuse;  /* 1: run each level's y-forward pass as its own launch instead of inside the
                        previous level's y-inverse pass */
 } hos_params;
