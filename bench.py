@@ -218,7 +218,7 @@ def run_ensemble(args, seed=0):
     fields, dts, hs = [], [], []
     for (n, M, kp, st, depth, sd) in specs:
         eta, phi, tp = jonswap_device(n, kp, st, sd, depth=depth)
-        f = HosField(n, n, order=M, precision="fp32", depth=depth, tune="auto")
+        f = HosField(n, n, order=M, precision="fp32", depth=depth)
         f._lib.hos_set_state_physical(f._h, _dptr(eta), _dptr(phi), 0.0)
         fields.append(f)
         dts.append(tp / 50)
