@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-configs", action="store_true")
     ap.add_argument("--ensemble-fields", type=int, default=256)
     ap.add_argument("--ensemble-steps", type=int, default=500)
     ap.add_argument("--serve-rate", type=float, default=1.2)
@@ -366,6 +367,45 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
+def run_configs(args):
+    """The 512^2, M = 4 configuration of the benchmark set on the same GPU:
+    a JONSWAP sea (kp = 16, kp*Hs/2 = 0.1, gamma = 3.3, s = 15, seed 2),
+    RK4 with dt = Tp/50, 1000 timed steps, once with the reference's dealias
+    rule (mx = floor(0.5 Nx/(1+0.5 L)) = 102) and once with the 2/3 rule
+    (mx = my = 170): steps/s of both forms, and the FP64 energy and volume
+    drift over the run."""
+    import torch
+
+    from hos_b200 import HosField, ic
+
+    out = []
+    eta, phi, info = ic.jonswap(512, 512, kp=16.0, steepness=0.1, gamma=3.3, spread_s=15.0, seed=2)
+    dt = info["Tp"] / 50
+    for rule, mx in (("reference rule, mx=102", None), ("2/3 rule, mx=my=170", 512 // 3)):
+        rec = {"workload": f"512x512 M=4 JONSWAP kp=16 kp*Hs/2=0.1 s=15, dealias {rule}", "steps": 1000}
+        for prec in ("fp64", "fp32"):
+            f = HosField(512, 512, order=4, precision=prec, mx=mx, my=mx)
+            f.set_state_physical(eta, phi)
+            v0 = f.volume()
+            f.step(dt, 5)
+            f.sync()
+            stream = torch.cuda.ExternalStream(f.stream)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            f.step(dt, 1000)
+            e1.record(stream)
+            f.sync()
+            rec[prec] = {"steps_per_s": 1000 / (e0.elapsed_time(e1) / 1e3)}
+            if prec == "fp64":
+                _, H = f.energy_history()
+                rec["fp64_energy_drift_rel"] = float(abs(H[-1] - H[0]) / abs(H[0]))
+                rec["fp64_volume_drift"] = float(abs(f.volume() - v0))
+            f.close()
+        out.append(rec)
+    return out
+
+
 # ------------------------------------------------------------------ our arm
 def run_ours(args, rep):
     import ctypes
@@ -512,6 +552,8 @@ def run_ours(args, rep):
         "gpu_launches": args.steps * f.launches_per_step,
         "clocks": clk,
     }
+    if not args.no_configs:
+        line["other_configs"] = run_configs(args)
     if not args.no_ensemble:
         ens = run_ensemble(args, seed=rank)
         line["ensemble"] = ens

@@ -142,7 +142,7 @@ def tune(nx, ny, order=5, precision="fp32", reps=3, use_cache=True, scales=(-1, 
         db[key] = {"tune": best, "report": report, "failed": failed}
         path = cache_path()
         os.makedirs(os.path.dirname(path), exist_ok=True)
-        tmp = path + ".tmp"
+        tmp = f"{path}.{os.getpid()}.tmp"  # concurrent ranks each write their own
         with open(tmp, "w") as fh:
             json.dump(db, fh, indent=1, sort_keys=True)
         os.replace(tmp, path)
