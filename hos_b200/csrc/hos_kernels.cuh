@@ -559,51 +559,60 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yinv(const __grid_constant__
     for (int e = 0; e < E; e++) po[t + e * P] = v[e];
   }
   if (MODE == YI_LEVEL && blockIdx.y == 0) {
-    // terms ordered by power 1, 2, ..., w_terms (host side); p = eta^k/k!
+    // W_n = own + sum_{p=1..w_terms} d_p eta^p/p! with own = d_z phi^(n+1)
+    // (this block's result) and w_in[q] the field of power q+1; then, when
+    // fused, P_(n+1) = -(own eta + sum_{p=2..nx_terms} d'_p eta^p/p!).  Both
+    // sums by Horner's rule from the highest power (acc = d_p + acc*eta/(p+1)).
     const C* pe = reinterpret_cast<const C*>(pall + (size_t)a.eta * psz + (size_t)ix * ny);
     C* pwo = reinterpret_cast<C*>(pall + (size_t)a.w_out * psz + (size_t)ix * ny);
-    C et[E], p[E];
-    C own[E];  // this block's result, d_z phi^(n+1)
+    C et[E], acc[E];
 #pragma unroll
-    for (int e = 0; e < E; e++) {
-      et[e] = pe[t + e * P];
-      p[e] = mkc((T)1, (T)1);
-      own[e] = v[e];
+    for (int e = 0; e < E; e++) et[e] = pe[t + e * P];
+    {
+      const C* pd = reinterpret_cast<const C*>(pall + (size_t)a.w_in[a.w_terms - 1] * psz + (size_t)ix * ny);
+#pragma unroll
+      for (int e = 0; e < E; e++) acc[e] = pd[t + e * P];
     }
-    for (int q = 0; q < a.w_terms; q++) {
+    for (int q = a.w_terms - 2; q >= 0; q--) {
       const C* pd = reinterpret_cast<const C*>(pall + (size_t)a.w_in[q] * psz + (size_t)ix * ny);
-      const T inv = (T)1 / (T)(q + 1);
+      const T inv = (T)1 / (T)(q + 2);
 #pragma unroll
       for (int e = 0; e < E; e++) {
         const C d = pd[t + e * P];
-        p[e].x = p[e].x * et[e].x * inv;
-        p[e].y = p[e].y * et[e].y * inv;
-        v[e].x += d.x * p[e].x;
-        v[e].y += d.y * p[e].y;
+        acc[e].x = d.x + acc[e].x * et[e].x * inv;
+        acc[e].y = d.y + acc[e].y * et[e].y * inv;
       }
     }
 #pragma unroll
-    for (int e = 0; e < E; e++) pwo[t + e * P] = v[e];
+    for (int e = 0; e < E; e++)
+      pwo[t + e * P] = mkc(v[e].x + acc[e].x * et[e].x, v[e].y + acc[e].y * et[e].y);
     if (a.fuse_next) {
-      // P_(n+1) (hosm_2d_par.c:302-317): the power-1 term is own * eta
+      // nx_in[q] holds the field of power q+1 for q >= 1; power 1 is own
+      if (a.nx_terms > 1) {
+        const C* pd = reinterpret_cast<const C*>(pall + (size_t)a.nx_in[a.nx_terms - 1] * psz + (size_t)ix * ny);
 #pragma unroll
-      for (int e = 0; e < E; e++) {
-        p[e] = et[e];
-        v[e].x = -own[e].x * et[e].x;
-        v[e].y = -own[e].y * et[e].y;
-      }
-      for (int q = 1; q < a.nx_terms; q++) {
-        const C* pd = reinterpret_cast<const C*>(pall + (size_t)a.nx_in[q] * psz + (size_t)ix * ny);
-        const T inv = (T)1 / (T)(q + 1);
+        for (int e = 0; e < E; e++) acc[e] = pd[t + e * P];
+        for (int q = a.nx_terms - 2; q >= 1; q--) {
+          const C* pq = reinterpret_cast<const C*>(pall + (size_t)a.nx_in[q] * psz + (size_t)ix * ny);
+          const T inv = (T)1 / (T)(q + 2);
+#pragma unroll
+          for (int e = 0; e < E; e++) {
+            const C d = pq[t + e * P];
+            acc[e].x = d.x + acc[e].x * et[e].x * inv;
+            acc[e].y = d.y + acc[e].y * et[e].y * inv;
+          }
+        }
 #pragma unroll
         for (int e = 0; e < E; e++) {
-          const C d = pd[t + e * P];
-          p[e].x = p[e].x * et[e].x * inv;
-          p[e].y = p[e].y * et[e].y * inv;
-          v[e].x -= d.x * p[e].x;
-          v[e].y -= d.y * p[e].y;
+          acc[e].x = v[e].x + acc[e].x * et[e].x * (T)0.5;
+          acc[e].y = v[e].y + acc[e].y * et[e].y * (T)0.5;
         }
+      } else {
+#pragma unroll
+        for (int e = 0; e < E; e++) acc[e] = v[e];
       }
+#pragma unroll
+      for (int e = 0; e < E; e++) v[e] = mkc(-acc[e].x * et[e].x, -acc[e].y * et[e].y);
     }
   }
   if (MODE == YI_LEVEL && a.fuse_next && blockIdx.y == 0)
@@ -703,27 +712,30 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yfwd(const __grid_constant__
 #pragma unroll
     for (int e = 0; e < E; e++) v[e] = src[t + e * P];
   } else if (MODE == YF_LEVEL) {
-    // terms are ordered by power 1, 2, ..., nterms (host side); pw = eta^p/p!
+    // P = -sum_{p=1..nterms} d_p eta^p/p! (t_in[q] holds the field of power
+    // q+1), by Horner's rule from the highest power: acc = d_n, acc = d_p +
+    // acc*eta/(p+1) down to p = 1, P = -acc*eta
     const C* pe = reinterpret_cast<const C*>(pall + (size_t)a.eta * psz + rowoff);
-    C et[E], pw[E];
+    C et[E];
 #pragma unroll
-    for (int e = 0; e < E; e++) {
-      et[e] = pe[t + e * P];
-      pw[e] = mkc((T)1, (T)1);
-      v[e] = mkc((T)0, (T)0);
+    for (int e = 0; e < E; e++) et[e] = pe[t + e * P];
+    {
+      const C* pd = reinterpret_cast<const C*>(pall + (size_t)a.t_in[a.nterms - 1] * psz + rowoff);
+#pragma unroll
+      for (int e = 0; e < E; e++) v[e] = pd[t + e * P];
     }
-    for (int q = 0; q < a.nterms; q++) {
+    for (int q = a.nterms - 2; q >= 0; q--) {
       const C* pd = reinterpret_cast<const C*>(pall + (size_t)a.t_in[q] * psz + rowoff);
-      const T inv = (T)1 / (T)(q + 1);
+      const T inv = (T)1 / (T)(q + 2);
 #pragma unroll
       for (int e = 0; e < E; e++) {
         const C d = pd[t + e * P];
-        pw[e].x = pw[e].x * et[e].x * inv;
-        pw[e].y = pw[e].y * et[e].y * inv;
-        v[e].x -= d.x * pw[e].x;
-        v[e].y -= d.y * pw[e].y;
+        v[e].x = d.x + v[e].x * et[e].x * inv;
+        v[e].y = d.y + v[e].y * et[e].y * inv;
       }
     }
+#pragma unroll
+    for (int e = 0; e < E; e++) v[e] = mkc(-v[e].x * et[e].x, -v[e].y * et[e].y);
   } else {
     const int which = blockIdx.y + a.which_base;
     const C* pex = reinterpret_cast<const C*>(pall + (size_t)a.ex * psz + rowoff);
