@@ -75,9 +75,13 @@ struct Dataset {
   uint64_t bytes = 0;
   const uint8_t* compact = nullptr;
   std::string unsupported;  // why the dataset cannot be read, if it cannot
+  // element count, or UNDEF if it overflows
   uint64_t count() const {
     uint64_t n = 1;
-    for (int i = 0; i < rank; i++) n *= dims[i];
+    for (int i = 0; i < rank; i++) {
+      if (dims[i] && n > UINT64_MAX / dims[i]) return UNDEF;
+      n *= dims[i];
+    }
     return n;
   }
 };
@@ -191,18 +195,22 @@ bool parse_messages(File& f, uint64_t start, uint64_t end, Dataset& d, uint64_t*
     const uint64_t sz = f.uint(a + 2, 2);
     const uint64_t m = a + 8;
     if (m + sz > end || !f.in(m, sz)) return f.bad("object header message out of bounds");
+    // every field read below lies inside the message's sz bytes
+    auto need = [&](uint64_t n) { return n <= sz; };
     switch (type) {
       case 0x0001: {  // dataspace
+        if (!need(4)) return f.bad("dataspace message too short");
         const int ver = f.p[m];
         d.rank = f.p[m + 1];
         if (d.rank > 8) return f.bad("dataspace rank above 8");
         const uint64_t dims_at = m + (ver == 1 ? 8 : 4);
-        if (!f.in(dims_at, (uint64_t)d.rank * f.sl)) return f.bad("dataspace truncated");
+        if (!need((ver == 1 ? 8 : 4) + (uint64_t)d.rank * f.sl)) return f.bad("dataspace truncated");
         if (ver == 2 && f.p[m + 3] == 2) d.rank = 0;  // null dataspace
         for (int i = 0; i < d.rank; i++) d.dims[i] = f.uint(dims_at + (uint64_t)i * f.sl, f.sl);
         break;
       }
       case 0x0003: {  // datatype
+        if (!need(8)) return f.bad("datatype message too short");
         const int cls = f.p[m] & 0x0f;
         const int bits0 = f.p[m + 1];
         d.size = (int)f.uint(m + 4, 4);
@@ -221,30 +229,38 @@ bool parse_messages(File& f, uint64_t start, uint64_t end, Dataset& d, uint64_t*
         break;
       }
       case 0x0008: {  // data layout
+        if (!need(2)) return f.bad("layout message too short");
         const int ver = f.p[m];
         if (ver == 3 || ver == 4) {
           d.layout = f.p[m + 1];
           if (d.layout == 0) {
+            if (!need(4)) return f.bad("layout message too short");
             d.bytes = f.uint(m + 2, 2);
+            if (!need(4 + d.bytes)) return f.bad("compact data outside its message");
             d.compact = f.p + m + 4;
           } else if (d.layout == 1) {
+            if (!need(2 + (uint64_t)f.so + f.sl)) return f.bad("layout message too short");
             d.addr = f.off(m + 2);
             d.bytes = f.uint(m + 2 + f.so, f.sl);
           } else {
             d.unsupported = "chunked or virtual storage";
           }
         } else if (ver == 1 || ver == 2) {
+          if (!need(8)) return f.bad("layout message too short");
           const int nd = f.p[m + 1];
           d.layout = f.p[m + 2];
-          uint64_t q = m + 8;
+          uint64_t q = 8;
           if (d.layout != 0) {
-            d.addr = f.off(q);
+            if (!need(q + f.so)) return f.bad("layout message too short");
+            d.addr = f.off(m + q);
             q += f.so;
           }
           q += 4ull * nd;
           if (d.layout == 0) {
-            d.bytes = f.uint(q, 4);
-            d.compact = f.p + q + 4;
+            if (!need(q + 4)) return f.bad("layout message too short");
+            d.bytes = f.uint(m + q, 4);
+            if (!need(q + 4 + d.bytes)) return f.bad("compact data outside its message");
+            d.compact = f.p + m + q + 4;
           } else if (d.layout != 1) {
             d.unsupported = "chunked storage";
           }
@@ -257,9 +273,11 @@ bool parse_messages(File& f, uint64_t start, uint64_t end, Dataset& d, uint64_t*
         d.unsupported = "filtered storage";
         break;
       case 0x0010:  // continuation
+        if (!need((uint64_t)f.so + f.sl)) return f.bad("continuation message too short");
         more.emplace_back(f.off(m) + f.base, f.uint(m + f.so, f.sl));
         break;
       case 0x0011:  // symbol table (a group)
+        if (!need(2ull * f.so)) return f.bad("symbol table message too short");
         *bt = f.off(m) + f.base;
         *hp = f.off(m + f.so) + f.base;
         break;
@@ -404,6 +422,7 @@ int hos_h5_info(const char* path, const char* name, int* rank, long long* dims, 
   if (!open_file(f, path)) return h5fail(path, "%s", f.err.c_str());
   const Dataset* d = find(f, name);
   if (!d) return h5fail(path, "no dataset '%s'", name);
+  if (d->rank > 4) return h5fail(path, "dataset '%s': rank %d (at most 4 supported)", name, d->rank);
   *rank = d->rank;
   for (int i = 0; i < d->rank && i < 4; i++) dims[i] = (long long)d->dims[i];
   if (type) {
@@ -422,6 +441,7 @@ int hos_h5_read_f64(const char* path, const char* name, double* out, long long n
   if (!d->unsupported.empty()) return h5fail(path, "dataset '%s': %s not supported", name, d->unsupported.c_str());
   if (d->cls < 0 || d->layout < 0) return h5fail(path, "dataset '%s' has no type or layout", name);
   const uint64_t n = d->count();
+  if (n == UNDEF || n > UINT64_MAX / (uint64_t)d->size) return h5fail(path, "dataset '%s': size overflows", name);
   if ((uint64_t)nelems != n) return h5fail(path, "dataset '%s' holds %llu elements, caller expects %lld", name,
                                            (unsigned long long)n, nelems);
   const uint64_t need = n * d->size;

@@ -151,3 +151,32 @@ def test_errors_are_reported(tmp_path):
         h5.write(tmp_path / "b.h5", {"a/b": 1.0})
     with pytest.raises(ValueError):
         h5.write(tmp_path / "c.h5", {"cube": np.zeros((2, 2, 2))})
+
+
+def test_damaged_files_fail_cleanly(tmp_path):
+    """Truncated files and flipped metadata bytes give an error or (when the
+    damage misses what a read needs) a result, never a crash."""
+    rng = np.random.default_rng(5)
+    good = tmp_path / "good.h5"
+    h5.write(good, {"a": rng.standard_normal((6, 5)), "n": np.int64(3), "s": 2.5})
+    raw = bytearray(open(good, "rb").read())
+    meta = min(len(raw), 3000)
+
+    def probe(path):
+        try:
+            for name in h5.names(path):
+                h5.read(path, name)
+        except (HosError, ValueError, MemoryError):
+            pass
+
+    for cut in range(0, len(raw), 41):
+        p = tmp_path / "cut.h5"
+        p.write_bytes(bytes(raw[:cut]))
+        probe(p)
+    for trial in range(300):
+        bad = bytearray(raw)
+        for _ in range(int(rng.integers(1, 4))):
+            bad[int(rng.integers(0, meta))] = int(rng.integers(0, 256))
+        p = tmp_path / "flip.h5"
+        p.write_bytes(bytes(bad))
+        probe(p)
