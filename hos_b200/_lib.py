@@ -47,6 +47,8 @@ class HosParams(ctypes.Structure):
         ("tune", ctypes.c_int * 8),
         ("tune_opb", ctypes.c_int),
         ("tune_nofuse", ctypes.c_int),
+        ("tune_ys", ctypes.c_int),
+        ("tune_sys", ctypes.c_int),
     ]
 
 

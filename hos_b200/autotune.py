@@ -20,8 +20,9 @@ import os
 KINDS = {  # tune index of E, tune index of the scale, pass names of the kind
     "xi": (0, 4, ("xinv_stage",)),
     "xf": (1, 5, ("xfwd_level", "xfwd_rhs")),
-    "yi": (2, 6, ("yinv_stage", "yinv_level")),
+    "yi": (2, 6, ("yinv_level",)),
     "yf": (3, 7, ("yfwd_level", "yfwd_rhs")),
+    "ys": (10, 11, ("yinv_stage",)),
 }
 
 
@@ -39,7 +40,7 @@ def _gpu_name():
 
 
 def _key(nx, ny, order, precision):
-    return f"step|{_gpu_name()}|{nx}x{ny}|M{order}|{precision}"
+    return f"step12|{_gpu_name()}|{nx}x{ny}|M{order}|{precision}"
 
 
 def _load():
@@ -62,12 +63,13 @@ def _valid_elems(precision, n):
 
 # The library's default shapes (ElemChoice / default_elems in hos_engine.cu):
 # E = 8 for every kind; lines-per-block scales xi, xf, yi, yf; all orders in
-# one block.
+# one block; levels fused; the stage y-inverse with E = 16, scale -1.  The 12 values
+# are hos_params.tune[8], tune_opb, tune_nofuse, tune_ys, tune_sys.
 DEFAULT_SCALES = {"fp32": (1, 0, 0, 0), "fp64": (-1, 0, -1, -1)}
 
 
 def default_tune(order, precision):
-    return [8, 8, 8, 8, *DEFAULT_SCALES[precision], order]
+    return [8, 8, 8, 8, *DEFAULT_SCALES[precision], order, 0, 16, -1]
 
 
 def _step_ms(field, dt, steps=20, reps=3):
@@ -90,7 +92,7 @@ def _step_ms(field, dt, steps=20, reps=3):
 
 
 def tune(nx, ny, order=5, precision="fp32", reps=3, use_cache=True, scales=(-1, 0, 1)):
-    """Return the 9 tune values (8 shapes, then orders per block) for
+    """Return the 12 tune values (see default_tune) for
     (nx, ny, order, precision), measuring and caching them if needed."""
     from . import ic
     from .field import HosField

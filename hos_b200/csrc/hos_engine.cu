@@ -252,6 +252,7 @@ struct ElemChoice {
   int xi = 8, xf = 8, yi = 8, yf = 8;          // elements per thread
   int sxi = 0, sxf = 0, syi = 0, syf = 0;      // lines per block scaled by 2^s
   int opb = 16;                                // z-derivative orders per block of the level x-forward pass (all)
+  int ys = 16, sys = -1;                       // E and scale of the stage y-inverse pass (YI_JOBS)
   int fuse = 1;                                // next level's y-forward inside each level's y-inverse
 };
 
@@ -274,6 +275,7 @@ struct PassCfg {
   YFwdFn yfwd_b[3] = {};
   ElemChoice ec;
   KindCfg xi, xf, yi, yf;
+  KindCfg ys;  // the stage y-inverse pass (YI_JOBS); yi is the level one
   const void* twx = nullptr;  // length nx
   const void* twh = nullptr;  // length ny/2
   const void* twy = nullptr;  // length ny
@@ -508,20 +510,22 @@ int make_cfg(hos_ctx* c, int prec, const ElemChoice& ec, PassCfg* o) {
   const size_t cs = prec ? sizeof(float2) : sizeof(double2);
   const int exi = pick_elems(prec, c->nx, ec.xi), exf = pick_elems(prec, c->nx, ec.xf);
   const int eyi = pick_elems(prec, c->h, ec.yi), eyf = pick_elems(prec, c->h, ec.yf);
+  const int eys = pick_elems(prec, c->h, ec.ys);
   for (int m = 0; m < 2; m++) o->xinv[m] = lookup_xinv(prec, m, c->nx, exi);
   for (int m = 0; m < 3; m++) o->xfwd[m] = lookup_xfwd(prec, m, c->nx, exf);
-  for (int m = 0; m < 2; m++) o->yinv[m] = lookup_yinv(prec, m, c->h, eyi);
+  for (int m = 0; m < 2; m++) o->yinv[m] = lookup_yinv(prec, m, c->h, m == YI_JOBS ? eys : eyi);
   for (int m = 0; m < 3; m++) o->yfwd[m] = lookup_yfwd(prec, m, c->h, eyf);
   for (int m = 0; m < 3; m++)
     if (!o->xfwd[m] || !o->yfwd[m] || (m < 2 && (!o->xinv[m] || !o->yinv[m])))
       return fail(HOS_ERR_ARG, "no kernels for %dx%d (E %d/%d/%d/%d)", c->nx, c->ny, exi, exf, eyi, eyf);
   for (int m = 0; m < 2; m++) o->xinv_b[m] = lookup_xinv(prec, m, c->nx, exi, true);
   for (int m = 0; m < 3; m++) o->xfwd_b[m] = lookup_xfwd(prec, m, c->nx, exf, true);
-  for (int m = 0; m < 2; m++) o->yinv_b[m] = lookup_yinv(prec, m, c->h, eyi, true);
+  for (int m = 0; m < 2; m++) o->yinv_b[m] = lookup_yinv(prec, m, c->h, m == YI_JOBS ? eys : eyi, true);
   for (int m = 0; m < 3; m++) o->yfwd_b[m] = lookup_yfwd(prec, m, c->h, eyf, true);
   o->ec = ec;
   if (x_geometry(c->nx, exi, cs, ec.sxi, &o->xi) || x_geometry(c->nx, exf, cs, ec.sxf, &o->xf) ||
-      y_geometry(c->h, c->nx, eyi, cs, ec.syi, &o->yi) || y_geometry(c->h, c->nx, eyf, cs, ec.syf, &o->yf))
+      y_geometry(c->h, c->nx, eyi, cs, ec.syi, &o->yi) || y_geometry(c->h, c->nx, eyf, cs, ec.syf, &o->yf) ||
+      y_geometry(c->h, c->nx, eys, cs, ec.sys, &o->ys))
     return fail(HOS_ERR_ARG, "no launch geometry for %dx%d", c->nx, c->ny);
   // The dynamic shared memory limit of a kernel is only ever raised: handles
   // with different shapes (and a handle's compute and boundary passes) share
@@ -538,11 +542,11 @@ int make_cfg(hos_ctx* c, int prec, const ElemChoice& ec, PassCfg* o) {
     std::lock_guard<std::mutex> lk(g_attr_mu);
     for (int m = 0; m < 2; m++) HOS_CK(raise((const void*)o->xinv[m], o->xi.smem));
     for (int m = 0; m < 3; m++) HOS_CK(raise((const void*)o->xfwd[m], o->xf.smem));
-    for (int m = 0; m < 2; m++) HOS_CK(raise((const void*)o->yinv[m], o->yi.smem));
+    for (int m = 0; m < 2; m++) HOS_CK(raise((const void*)o->yinv[m], m == YI_JOBS ? o->ys.smem : o->yi.smem));
     for (int m = 0; m < 3; m++) HOS_CK(raise((const void*)o->yfwd[m], o->yf.smem));
     for (int m = 0; m < 2; m++) HOS_CK(raise((const void*)o->xinv_b[m], o->xi.smem));
     for (int m = 0; m < 3; m++) HOS_CK(raise((const void*)o->xfwd_b[m], o->xf.smem));
-    for (int m = 0; m < 2; m++) HOS_CK(raise((const void*)o->yinv_b[m], o->yi.smem));
+    for (int m = 0; m < 2; m++) HOS_CK(raise((const void*)o->yinv_b[m], m == YI_JOBS ? o->ys.smem : o->yi.smem));
     for (int m = 0; m < 3; m++) HOS_CK(raise((const void*)o->yfwd_b[m], o->yf.smem));
   }
   o->twx = c->tw[prec][0];
@@ -665,10 +669,10 @@ void build_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, doub
   PassRec r2;
   r2.kind = L_YINV;
   r2.mode = YI_JOBS;
-  r2.gx = ygrid(c, g.yi);
+  r2.gx = ygrid(c, g.ys);
   YInvArgs& ya = r2.yi;
   ya.geo = c->geo;
-  ya.lp = g.yi.lp;
+  ya.lp = g.ys.lp;
   ya.z = c->zbuf;
   ya.rows_in = c->h + 1;
   ya.rows_dev = rows_dev;
@@ -905,7 +909,11 @@ void launch_single(hos_ctx* c, const PassRec& r) {
   switch (r.kind) {
     case L_XINV: launch_pdl(g.xinv[r.mode], grid, g.xi.threads, g.xi.smem, c->st, r.xi, nxi, twx); break;
     case L_XFWD: launch_pdl(g.xfwd[r.mode], grid, g.xf.threads, g.xf.smem, c->st, r.xf, nxf, twx); break;
-    case L_YINV: launch_pdl(g.yinv[r.mode], grid, g.yi.threads, g.yi.smem, c->st, r.yi, nyi, twh, twy); break;
+    case L_YINV: {
+      const KindCfg& k = r.mode == YI_JOBS ? g.ys : g.yi;
+      launch_pdl(g.yinv[r.mode], grid, k.threads, k.smem, c->st, r.yi, nyi, twh, twy);
+      break;
+    }
     default: launch_pdl(g.yfwd[r.mode], grid, g.yf.threads, g.yf.smem, c->st, r.yf, nyf, twh, twy); break;
   }
 }
@@ -993,13 +1001,13 @@ int enqueue_c2r(hos_ctx* c, const double2* spec_in, double* phys_out) {
   g.xinv[XI_PLAIN]<<<dim3(xgrid(c, g.xi), 1), g.xi.threads, g.xi.smem, c->st>>>(xa, nullptr, g.twx);
   YInvArgs ya{};
   ya.geo = c->geo;
-  ya.lp = g.yi.lp;
+  ya.lp = g.ys.lp;
   ya.z = c->zplain;
   ya.rows_in = c->h + 1;
   ya.phys = phys_out;
   ya.jobs[0] = YJob{0, 0, 0};
   ya.ycount = 1;
-  g.yinv[YI_JOBS]<<<dim3(ygrid(c, g.yi), 1), g.yi.threads, g.yi.smem, c->st>>>(ya, nullptr, g.twh, g.twy);
+  g.yinv[YI_JOBS]<<<dim3(ygrid(c, g.ys), 1), g.ys.threads, g.ys.smem, c->st>>>(ya, nullptr, g.twh, g.twy);
   return HOS_OK;
 }
 
@@ -1093,6 +1101,7 @@ bool same_class(const hos_ctx* a, const hos_ctx* b) {
          a->cfg.ec.xi == b->cfg.ec.xi && a->cfg.ec.xf == b->cfg.ec.xf && a->cfg.ec.yi == b->cfg.ec.yi &&
          a->cfg.ec.yf == b->cfg.ec.yf && a->cfg.ec.sxi == b->cfg.ec.sxi && a->cfg.ec.sxf == b->cfg.ec.sxf &&
          a->cfg.ec.syi == b->cfg.ec.syi && a->cfg.ec.syf == b->cfg.ec.syf && a->cfg.ec.opb == b->cfg.ec.opb && a->cfg.ec.fuse == b->cfg.ec.fuse &&
+         a->cfg.ec.ys == b->cfg.ec.ys && a->cfg.ec.sys == b->cfg.ec.sys &&
          a->device == b->device;
 }
 
@@ -1207,7 +1216,9 @@ int build_ens_graph(hos_ens* E) {
           g.xfwd_b[b.mode]<<<grid, g.xf.threads, g.xf.smem, K.st>>>(XFwdArgs{}, (const XFwdArgs*)a, g.twx);
           break;
         case L_YINV:
-          g.yinv_b[b.mode]<<<grid, g.yi.threads, g.yi.smem, K.st>>>(YInvArgs{}, (const YInvArgs*)a, g.twh, g.twy);
+          g.yinv_b[b.mode]<<<grid, b.mode == YI_JOBS ? g.ys.threads : g.yi.threads,
+                             b.mode == YI_JOBS ? g.ys.smem : g.yi.smem, K.st>>>(YInvArgs{}, (const YInvArgs*)a, g.twh,
+                                                                                  g.twy);
           break;
         default:
           g.yfwd_b[b.mode]<<<grid, g.yf.threads, g.yf.smem, K.st>>>(YFwdArgs{}, (const YFwdArgs*)a, g.twh, g.twy);
@@ -1380,6 +1391,13 @@ int hos_create(const hos_params* p, hos_handle* out) {
       ec.syf = clamp3(p->tune[7]);
     }
     if (p->tune_opb > 0) ec.opb = p->tune_opb;
+    if (p->tune_ys) {  // the stage y-inverse tuned on its own; otherwise it follows the level one
+      ec.ys = p->tune_ys;
+      ec.sys = clamp3(p->tune_sys);
+    } else if (tuned) {
+      ec.ys = ec.yi;
+      ec.sys = ec.syi;
+    }
     if (p->tune_nofuse) ec.fuse = 0;
     rc = make_cfg(c, c->prec, ec, &c->cfg);
     if (!rc) rc = make_cfg(c, 0, ec64, &c->cfg64);

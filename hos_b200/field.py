@@ -81,6 +81,8 @@ class HosField:
                 p.tune_opb = int(tv[8])
             if len(tv) > 9:
                 p.tune_nofuse = int(tv[9])
+            if len(tv) > 11:
+                p.tune_ys, p.tune_sys = int(tv[10]), int(tv[11])
         self.params = p
         self.nx, self.ny, self.h = int(nx), int(ny), int(ny) // 2
         h = ctypes.c_void_p()

@@ -12,7 +12,7 @@ import sys
 
 from . import HosField, ic
 
-TUNED = {"fp32": [8, 8, 8, 8, 1, 0, 0, 0, 5], "fp64": [8, 8, 8, 8, -1, 0, -1, -1, 5]}
+TUNED = {"fp32": [8, 8, 8, 8, 1, 0, 0, 0, 5, 0, 16, -1], "fp64": [8, 8, 8, 8, -1, 0, -1, -1, 5, 0, 16, -1]}
 
 
 def main(argv):

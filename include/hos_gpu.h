@@ -64,11 +64,13 @@ typedef struct hos_params {
   int scheme;       /* HOS_RK4 etc. */
   int mx, my;       /* dealias bounds; 0 selects the reference rule (operators_par.c:290-291) */
   int tune[8];      /* kernel shapes (0 = default): elements per thread of the x-inverse, x-forward,
-                       y-inverse and y-forward passes (8, 16, or 32 in FP32), then the base-2 exponents
+                       (level) y-inverse and y-forward passes (8, 16, or 32 in FP32), then the base-2 exponents
                        scaling their lines per block; chosen by hos_b200.autotune */
   int tune_opb;     /* z-derivative orders per block of the level x-forward pass (0 = all in one block) */
   int tune_nofuse;  /* 1: run each level's y-forward pass as its own launch instead of inside the
                        previous level's y-inverse pass */
+  int tune_ys;      /* elements per thread of the stage y-inverse pass (0: as the level y-inverse, tune[2]) */
+  int tune_sys;     /* its lines-per-block exponent (used when tune_ys is set) */
 } hos_params;
 
 typedef struct hos_ctx* hos_handle;
