@@ -167,7 +167,9 @@ def ncu_traffic():
 
 
 def algorithmic_step_bytes(n, order, prec_bytes):
-    """Survey byte model per RK4 step: 4*T_M*(R_p + C_p) + 26*C_64."""
+    """Algorithmic bytes per RK4 step, 4*T_M*(R_p + C_p) + 26*C_64: each of the
+    T_M transforms of the 4 RHS evaluations reads its input once and writes
+    its output once, plus the FP64 state traffic of the stages."""
     tm = 6 + order + order * (order + 1) // 2
     R = n * n * prec_bytes
     C = n * (n // 2 + 1) * 2 * prec_bytes

@@ -70,7 +70,7 @@ def test_stokes_100_rk4_steps_drop_in_gate(golden):
         eta, phi = f.state_physical()
     assert rel(u[0], d["u100"][0]) < TOL_STEPS
     assert rel(u[1], d["u100"][1]) < TOL_STEPS
-    # physical eta, phi_s as the survey's parity metric states it
+    # the parity metric is stated on physical eta and phi_s
     assert rel(eta, hn.ifft2(d["u100"][0])) < TOL_STEPS
     assert rel(phi, hn.ifft2(d["u100"][1])) < TOL_STEPS
     assert abs(t - float(d["t100"])) < 1e-12
