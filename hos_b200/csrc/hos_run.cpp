@@ -19,8 +19,9 @@
 //
 // The reference fixes three values in its source: the HOS order (NLevs = 2,
 // euler_2d_par.h:24, so M = 3), the scheme (4, midpoint RK2,
-// main_2d_par.c:252) and dt (0.2, :302).  They are the defaults here and
-// options change them:
+// main_2d_par.c:252) and dt (0.2, :302).  They are the defaults here; the
+// optional datasets /M, /scheme and /dt of initpars.h5 replace them, and the
+// options replace both:
 //   hos_run [-M order] [-dt dt] [-scheme 1..5] [-fp32] [-C dir] [-q]
 #include <unistd.h>
 
@@ -46,6 +47,14 @@ bool quiet = false;
 
 void ck(int rc, const char* what) {
   if (rc != HOS_OK) die(what);
+}
+
+// Whether the file holds a dataset of that name (errors reading the file
+// itself surface at the first required read).
+bool has(const char* file, const char* name) {
+  int rank = 0, type = 0;
+  long long dims[4] = {0, 0, 0, 0};
+  return hos_h5_info(file, name, &rank, dims, &type) == HOS_OK;
 }
 
 double scalar(const char* file, const char* name) {
@@ -129,6 +138,7 @@ struct Runtime {
 int main(int argc, char** argv) {
   int order = 3, scheme = 4, prec = HOS_PREC_FP64;
   double dt = 0.2;
+  bool set_order = false, set_scheme = false, set_dt = false;
   for (int i = 1; i < argc; i++) {
     const std::string a = argv[i];
     auto next = [&]() -> const char* {
@@ -140,10 +150,13 @@ int main(int argc, char** argv) {
     };
     if (a == "-M") {
       order = atoi(next());
+      set_order = true;
     } else if (a == "-dt") {
       dt = atof(next());
+      set_dt = true;
     } else if (a == "-scheme") {
       scheme = atoi(next());
+      set_scheme = true;
     } else if (a == "-fp32") {
       prec = HOS_PREC_FP32;
     } else if (a == "-C") {
@@ -157,10 +170,6 @@ int main(int argc, char** argv) {
       fprintf(stderr, "usage: hos_run [-M order] [-dt dt] [-scheme 1..5] [-fp32] [-C dir] [-q]\n");
       return EXIT_FAILURE;
     }
-  }
-  if (!(dt > 0)) {
-    fprintf(stderr, "hos_run: dt must be positive\n");
-    return EXIT_FAILURE;
   }
 
   Runtime rt;
@@ -183,6 +192,13 @@ int main(int argc, char** argv) {
     rampflg = 0;
   }
   const double tramp = scalar(pars, "Tramp");
+  if (!set_order && has(pars, "M")) order = (int)scalar(pars, "M");
+  if (!set_scheme && has(pars, "scheme")) scheme = (int)scalar(pars, "scheme");
+  if (!set_dt && has(pars, "dt")) dt = scalar(pars, "dt");
+  if (!(dt > 0)) {
+    fprintf(stderr, "hos_run: dt must be positive\n");
+    return EXIT_FAILURE;
+  }
 
   // file names: the reference formats runsubid into 2 bytes (one digit) and
   // the snapshot number into 5 (main_2d_par.c:45,93,112)

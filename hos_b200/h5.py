@@ -27,7 +27,7 @@ F64, F32, I64, I32 = 0, 1, 2, 3
 # plus KP and h, which write_hdf5.py stores and the C code does not read.
 # Counts and flags are stored as int64; the other values as h5py stores the
 # Python value given (int64 for an int, float64 for a float).
-INT_PARAMS = ("Nx", "Ny", "KP", "saveflg", "runsubid", "rampflg")
+INT_PARAMS = ("Nx", "Ny", "KP", "saveflg", "runsubid", "rampflg", "M", "scheme")
 REQUIRED_PARAMS = ("Nx", "Ny", "Lx", "Ly", "g", "runsubid", "T", "dtsave", "saveflg", "rampflg", "Tramp")
 
 
@@ -109,7 +109,7 @@ def read_params(path):
         if k not in present:
             raise KeyError(f"{path}: parameter dataset /{k} missing")
         p[k] = float(read(path, k).reshape(-1)[0])
-    for k in ("KP", "h"):
+    for k in ("KP", "h", "M", "scheme", "dt"):  # the last three: hos_run's optional run settings
         if k in present:
             p[k] = float(read(path, k).reshape(-1)[0])
     for k in ("Nx", "Ny", "runsubid", "saveflg", "rampflg"):
@@ -122,16 +122,21 @@ def read_params(path):
 
 
 def write_inputs(folder, eta, phi, lx, ly, g, T, dtsave, runsubid=1, saveflg=1, rampflg=1, tramp=200, h=1000.0,
-                 kp=10000, bathy=None):
+                 kp=10000, bathy=None, order=None, scheme=None, dt=None):
     """initpars.h5 and initdata.<runsubid>.h5 in `folder`, holding what the
     reference's python/write_hdf5.py:5-40 writes (the file names are the
-    ones main_2d_par.c:80-100 opens)."""
+    ones main_2d_par.c:80-100 opens).  order, scheme and dt, when given, are
+    stored as /M, /scheme and /dt, which hos_run reads in place of the
+    values the reference compiles in (M = 3, scheme 4, dt = 0.2)."""
     eta = np.asarray(eta, dtype=np.float64)
     phi = np.asarray(phi, dtype=np.float64)
     nx, ny = eta.shape
     bathy = np.zeros_like(eta) if bathy is None else np.asarray(bathy, dtype=np.float64)
     vals = {"Nx": nx, "Ny": ny, "Lx": lx, "Ly": ly, "g": g, "KP": kp, "h": h, "T": T, "dtsave": dtsave,
             "saveflg": saveflg, "runsubid": runsubid, "rampflg": rampflg, "Tramp": tramp}
+    for k, v in (("M", order), ("scheme", scheme), ("dt", dt)):
+        if v is not None:
+            vals[k] = v
     types = {k: I64 if k in INT_PARAMS or isinstance(v, (int, np.integer)) else F64 for k, v in vals.items()}
     os.makedirs(folder, exist_ok=True)
     write(os.path.join(folder, "initpars.h5"), vals, types)

@@ -135,6 +135,28 @@ def test_hos_run_driver_matches_reference(tmp_path):
     assert h5.read(tmp_path / "data_coordinates.h5", "xy").shape == (n * n, 2)
 
 
+def test_hos_run_takes_order_scheme_dt_from_the_parameter_file(tmp_path):
+    n, lx, g = 64, 1000.0, 9.81
+    eta, phi, info = ic.jonswap(n, n, lx=lx, ly=lx, g=g, kp=2 * math.pi / lx * 6, steepness=0.08, seed=10)
+    h5.write_inputs(tmp_path, eta, phi, lx, lx, g, T=1, dtsave=1.0, runsubid=1, saveflg=1, rampflg=0, tramp=1,
+                    order=4, scheme=2, dt=0.1)
+    assert h5.read_params(tmp_path / "initpars.h5")["M"] == 4.0
+    r = subprocess.run([HOS_RUN, "-C", str(tmp_path), "-q"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    ora = _Oracle(4, n, lx, g, 0, 1.0, 2)
+    u, t, H = ora.steps(ora.init(eta, phi), 0.0, 0.1, 10)
+    assert h5.read(tmp_path / "data1.1.h5", "time")[0, 0] == t
+    assert rel(h5.read(tmp_path / "data1.1.h5", "eta"), ora.ifft2(u[0])) < TOL
+    assert len((tmp_path / "runtime.dat").read_text().splitlines()) == 10
+    # the command line overrides the file
+    r = subprocess.run([HOS_RUN, "-C", str(tmp_path), "-q", "-M", "3", "-dt", "0.2"], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr
+    ora3 = _Oracle(3, n, lx, g, 0, 1.0, 2)
+    u3, t3, _ = ora3.steps(ora3.init(eta, phi), 0.0, 0.2, 5)
+    assert rel(h5.read(tmp_path / "data1.1.h5", "eta"), ora3.ifft2(u3[0])) < TOL
+
+
 def test_hos_run_reports_missing_input(tmp_path):
     r = subprocess.run([HOS_RUN, "-C", str(tmp_path), "-q"], capture_output=True, text=True, timeout=60)
     assert r.returncode != 0 and "initpars.h5" in r.stderr
