@@ -46,6 +46,13 @@ struct Legacy {
   hos_params p{};
   int scheme = HOS_MIDPOINT;  // main_2d_par.c:252 uses scheme 4
   int nlevs = -1;             // NLevs, euler_2d_par.h:24
+  // Resident mode: the state sol_update_RK advanced stays on the device; the
+  // host array `resident` is brought up to date only when a call here reads
+  // it (host_stale) and is re-uploaded after a call here writes it.
+  int resident_mode = -1;     // -1: not yet read from HOS_LEGACY_RESIDENT
+  double* resident = nullptr;
+  bool host_stale = false;
+  double dev_t = 0.0;         // the device's time after the last step
 };
 Legacy L;
 std::mutex mu;
@@ -60,6 +67,42 @@ int nlevs_now() {
 
 void report(const char* where) {
   fprintf(stderr, "libhos_gpu %s: %s\n", where, hos_last_error());
+}
+
+size_t field() { return (size_t)Nx * (size_t)(Ny / 2 + 1); }
+
+bool resident_mode() {
+  if (L.resident_mode < 0) {
+    const char* s = getenv("HOS_LEGACY_RESIDENT");
+    L.resident_mode = (s && s[0] == '1') ? 1 : 0;
+  }
+  return L.resident_mode == 1;
+}
+
+// Brings the host copy of the resident state up to date.
+void sync_host(const char* where) {
+  if (!L.host_stale || !L.h || !L.resident) return;
+  if (hos_get_state_spectral(L.h, L.resident, nullptr) != HOS_OK) report(where);
+  L.host_stale = false;
+}
+
+// Whether p points into the resident packed state (both fields).
+bool in_state(const void* p) {
+  if (!L.resident || !p) return false;
+  const double* q = static_cast<const double*>(p);
+  return q >= L.resident && q < L.resident + 4 * field();
+}
+
+// Before a call reads the host array p.
+void reading(const void* p, const char* where) {
+  if (in_state(p)) sync_host(where);
+}
+
+// Before a call writes the host array p: the host copy becomes the newer one.
+void writing(const void* p, const char* where) {
+  if (!in_state(p)) return;
+  sync_host(where);
+  L.resident = nullptr;
 }
 
 // The context for the current globals, created or re-created on change.
@@ -81,6 +124,8 @@ hos_handle ctx(const char* where) {
     return nullptr;
   }
   if (L.h && memcmp(&p, &L.p, sizeof(p)) == 0) return L.h;
+  sync_host(where);  // the old context holds the newest state
+  L.resident = nullptr;
   if (L.h) hos_destroy(L.h);
   L.h = nullptr;
   if (hos_create(&p, &L.h) != HOS_OK) {
@@ -91,8 +136,6 @@ hos_handle ctx(const char* where) {
   L.p = p;
   return L.h;
 }
-
-size_t field() { return (size_t)Nx * (size_t)(Ny / 2 + 1); }
 
 }  // namespace
 
@@ -113,8 +156,22 @@ void rhs_hos_setup(void) {
   ctx("rhs_hos_setup");
 }
 
+void hos_legacy_set_resident(int on) {
+  std::lock_guard<std::mutex> lk(mu);
+  sync_host("hos_legacy_set_resident");
+  L.resident = nullptr;
+  L.resident_mode = on ? 1 : 0;
+}
+
+void hos_legacy_sync(void) {
+  std::lock_guard<std::mutex> lk(mu);
+  sync_host("hos_legacy_sync");
+}
+
 void rhs_hos_clean(void) {
   std::lock_guard<std::mutex> lk(mu);
+  sync_host("rhs_hos_clean");
+  L.resident = nullptr;
   if (L.h) hos_destroy(L.h);
   L.h = nullptr;
 }
@@ -124,8 +181,27 @@ void sol_update_RK(double* u, double* t, double dt, char* dtflag) {
   std::lock_guard<std::mutex> lk(mu);
   hos_handle h = ctx("sol_update_RK");
   if (!h) return;
-  if (hos_set_state_spectral(h, u, *t) || hos_clear_history(h) || hos_step(h, dt, 1) ||
-      hos_get_state_spectral(h, u, nullptr)) {
+  const bool keep = resident_mode();
+  // the state on the device is current when it is this array's, advanced by
+  // our last step to the caller's time
+  const bool on_device = keep && L.resident == u && L.dev_t == *t;
+  if (!on_device) {
+    sync_host("sol_update_RK");
+    L.resident = nullptr;
+    if (hos_set_state_spectral(h, u, *t)) {
+      report("sol_update_RK");
+      return;
+    }
+  }
+  if (hos_clear_history(h) || hos_step(h, dt, 1)) {
+    report("sol_update_RK");
+    return;
+  }
+  if (keep) {
+    L.resident = u;
+    L.host_stale = true;
+    L.dev_t = *t + dt;  // the device advances t exactly so (time_schemes_par.c:119)
+  } else if (hos_get_state_spectral(h, u, nullptr)) {
     report("sol_update_RK");
     return;
   }
@@ -148,6 +224,8 @@ void sol_update_RK(double* u, double* t, double dt, char* dtflag) {
 void rhs_hos(double* hrhs, double* hu, double t) {
   std::lock_guard<std::mutex> lk(mu);
   hos_handle h = ctx("rhs_hos");
+  reading(hu, "rhs_hos");
+  writing(hrhs, "rhs_hos");
   if (h && hos_rhs(h, hu, hrhs, t)) report("rhs_hos");
 }
 
@@ -155,6 +233,8 @@ void rhs_test(double* hrhs, double* hu) {
   std::lock_guard<std::mutex> lk(mu);
   hos_handle h = ctx("rhs_test");
   if (!h) return;
+  reading(hu, "rhs_test");
+  writing(hrhs, "rhs_test");
   const size_t f = field();
   if (hos_spectral_op(h, HOS_OP_DX, hu, nullptr, hrhs) ||
       hos_spectral_op(h, HOS_OP_DY, hu + 2 * f, nullptr, hrhs + 2 * f))
@@ -165,18 +245,25 @@ void Zvel(double* hu, double* hZvelM, double* hZvelM2, double* hZvel2M, double* 
   (void)t;
   std::lock_guard<std::mutex> lk(mu);
   hos_handle h = ctx("Zvel");
+  reading(hu, "Zvel");
+  for (double* o : {hZvelM, hZvelM2, hZvel2M, hZvel2M2}) writing(o, "Zvel");
   if (h && hos_zvel(h, hu, hZvelM, hZvelM2, hZvel2M, hZvel2M2)) report("Zvel");
 }
 
 void ZvelLinear(const double* hu, double* hZvelLinear) {
   std::lock_guard<std::mutex> lk(mu);
   hos_handle h = ctx("ZvelLinear");
+  reading(hu, "ZvelLinear");
+  writing(hZvelLinear, "ZvelLinear");
   if (h && hos_spectral_op(h, HOS_OP_DZ, hu + 2 * field(), nullptr, hZvelLinear)) report("ZvelLinear");
 }
 
 double Hamiltonian(const double* heta, const double* heta_t, const double* hphi) {
   std::lock_guard<std::mutex> lk(mu);
   hos_handle h = ctx("Hamiltonian");
+  reading(heta, "Hamiltonian");
+  reading(heta_t, "Hamiltonian");
+  reading(hphi, "Hamiltonian");
   double H = 0.0;
   if (h && hos_hamiltonian(h, heta, heta_t, hphi, &H)) report("Hamiltonian");
   return H;
@@ -187,6 +274,9 @@ double RampFun(const double t) { return 1 - exp(-t * t / Tramp / Tramp); }  // h
 static void op1(int op, const double* a, const double* b, double* out, const char* where) {
   std::lock_guard<std::mutex> lk(mu);
   hos_handle h = ctx(where);
+  reading(a, where);
+  reading(b, where);
+  writing(out, where);
   if (h && hos_spectral_op(h, op, a, b, out)) report(where);
 }
 
@@ -201,6 +291,7 @@ void fft_2d(double* u, double* hu, void* plan) {
   (void)plan;
   std::lock_guard<std::mutex> lk(mu);
   hos_handle h = ctx("fft_2d");
+  writing(hu, "fft_2d");
   if (h && hos_fft_2d_ld(h, u, Ny + 2, hu)) report("fft_2d");
 }
 
@@ -208,6 +299,7 @@ void ifft_2d(double* hu, double* u, void* plan) {
   (void)plan;
   std::lock_guard<std::mutex> lk(mu);
   hos_handle h = ctx("ifft_2d");
+  reading(hu, "ifft_2d");
   if (h && hos_ifft_2d_ld(h, hu, u, Ny + 2)) report("ifft_2d");
 }
 

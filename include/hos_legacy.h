@@ -26,7 +26,7 @@
  *
  * Arrays are host memory.  sol_update_RK uploads the state, advances one
  * step on the GPU and downloads it (the state is correct on the host after
- * every call).  Errors are recorded for hos_last_error(); the functions
+ * every call), unless resident mode (below) keeps it on the GPU.  Errors are recorded for hos_last_error(); the functions
  * return void, as the reference's do.
  */
 #ifndef HOS_LEGACY_H
@@ -82,6 +82,19 @@ void ifft_2d(double* hu, double* u, void* plan);
 
 /* Sets the HOS order of the legacy context (NLevs = M - 1, default 2). */
 void hos_legacy_set_nlevs(int nlevs);
+
+/* Resident mode (off by default; on with hos_legacy_set_resident(1) or
+ * HOS_LEGACY_RESIDENT=1 in the environment): the state array passed to
+ * sol_update_RK stays on the GPU between calls instead of being uploaded and
+ * downloaded every step.  The host array is brought up to date when one of
+ * the functions here reads it (ifft_2d at a save, Hamiltonian, Zvel, ...),
+ * at rhs_hos_clean() and by hos_legacy_sync(); a function here that writes
+ * into it (Dealias, fft_2d, ...) makes the host copy the one the next step
+ * uploads.  The reference's driver reads the state only through ifft_2d
+ * (main_2d_par.c:310-311), so it can run in this mode unchanged; code that
+ * reads the array directly calls hos_legacy_sync() first. */
+void hos_legacy_set_resident(int on);
+void hos_legacy_sync(void);
 
 #ifdef __cplusplus
 }

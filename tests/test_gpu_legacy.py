@@ -37,7 +37,7 @@ def lib():
         "Zvel": [P, P, P, P, P, ctypes.c_double], "ZvelLinear": [P, P], "Hamiltonian": [P, P, P],
         "RampFun": [ctypes.c_double], "Dx": [P, P], "Dy": [P, P], "Dz": [P, P], "Mult": [P, P, P],
         "Sum": [P, P, P], "Dealias": [P], "fft_2d": [P, P, P], "ifft_2d": [P, P, P],
-        "hos_legacy_set_nlevs": [ctypes.c_int],
+        "hos_legacy_set_nlevs": [ctypes.c_int], "hos_legacy_set_resident": [ctypes.c_int], "hos_legacy_sync": [],
     }.items():
         getattr(L, name).argtypes = args
     L.Hamiltonian.restype = ctypes.c_double
@@ -120,6 +120,56 @@ def test_driver_sequence_matches_reference(lib, tmp_path, monkeypatch):
     lib.ifft_2d(p(u[0]), p(back), None)
     assert rel(back[:, :ny], ref.ifft2(u_ref[0])) < 1e-10
     lib.rhs_hos_clean()
+
+
+def test_resident_state_between_steps(lib, tmp_path, monkeypatch):
+    """Resident mode: the state stays on the GPU across sol_update_RK calls
+    (the host array is not touched), a save through ifft_2d sees the current
+    state, an in-place Dealias between steps is taken up by the next step, and
+    hos_legacy_sync brings the host array up to date; all as the reference's
+    code computes it."""
+    if not ref_c.available(3):
+        pytest.skip("C oracle not built")
+    monkeypatch.chdir(tmp_path)
+    nx, ny, M, dt = 64, 64, 3, 0.2
+    lx, g, tramp = 600.0, 9.81, 1.0
+    eta, phi, _ = ic.jonswap(nx, ny, lx=lx, ly=lx, g=g, kp=2 * math.pi / lx * 6, steepness=0.08, seed=23)
+    set_globals(lib, nx, ny, lx, lx, g, 1, tramp, "runtime.dat")
+    lib.hos_legacy_set_nlevs(M - 1)
+    lib.Setup_TimeScheme(4)
+    lib.rhs_hos_setup()
+    lib.hos_legacy_set_resident(1)
+    try:
+        u = np.zeros((2, ny // 2 + 1, nx), complex)
+        e_p, f_p = padded(eta), padded(phi)  # held: the library reads them during the calls
+        lib.fft_2d(p(e_p), p(u[0]), None)
+        lib.fft_2d(p(f_p), p(u[1]), None)
+        lib.Dealias(p(u[0]))
+        lib.Dealias(p(u[1]))
+        ref = ref_c.RefC(M, nx, ny, lx=lx, ly=lx, g=g, rampflg=1, tramp=tramp, scheme=4)
+        u_ref = ref.init_state(eta, phi)
+        u0 = u.copy()
+        t = np.zeros(1)
+        for _ in range(5):
+            lib.sol_update_RK(p(u), p(t), dt, None)
+        assert np.array_equal(u, u0)  # still on the GPU
+        u_ref, t_ref, _ = ref.steps(u_ref, 0.0, dt, 5)
+        back = np.zeros((nx, ny + 2))
+        lib.ifft_2d(p(u[0]), p(back), None)  # the save path syncs the host copy first
+        assert rel(back[:, :ny], ref.ifft2(u_ref[0])) < 1e-10
+        assert rel(u[1], u_ref[1]) < 1e-10
+        # a write between steps: Dealias(phi) in place (the identity on a dealiased state)
+        lib.Dealias(p(u[1]))
+        for _ in range(5):
+            lib.sol_update_RK(p(u), p(t), dt, None)
+        u_ref, t_ref, _ = ref.steps(u_ref, t_ref, dt, 5)
+        lib.hos_legacy_sync()
+        assert rel(u[0], u_ref[0]) < 1e-10 and rel(u[1], u_ref[1]) < 1e-10
+        assert abs(t[0] - t_ref) < 1e-15
+        assert len(open("runtime.dat").read().split("\n")[:-1]) == 10
+    finally:
+        lib.hos_legacy_set_resident(0)
+        lib.rhs_hos_clean()
 
 
 def test_operators_match_reference(lib, tmp_path, monkeypatch):
