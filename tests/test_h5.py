@@ -180,3 +180,21 @@ def test_damaged_files_fail_cleanly(tmp_path):
         p = tmp_path / "flip.h5"
         p.write_bytes(bytes(bad))
         probe(p)
+
+
+def test_run_inputs_round_trip(tmp_path):
+    """write_inputs stores what the reference's write_hdf5.py stores, plus the
+    optional run settings hos_run reads (/M, /scheme, /dt); read_params gives
+    them back as get_params would (all read as double)."""
+    rng = np.random.default_rng(9)
+    eta, phi = rng.standard_normal((8, 16)), rng.standard_normal((8, 16))
+    h5.write_inputs(tmp_path, eta, phi, 100.0, 50.0, 9.81, T=12, dtsave=0.5, runsubid=3, saveflg=2, rampflg=1,
+                    tramp=20, order=5, scheme=2, dt=0.05)
+    p = h5.read_params(tmp_path / "initpars.h5")
+    assert (p["Nx"], p["Ny"], p["runsubid"], p["saveflg"]) == (8, 16, 3, 2)
+    assert (p["M"], p["scheme"], p["dt"], p["T"], p["dtsave"]) == (5.0, 2.0, 0.05, 12.0, 0.5)
+    assert h5.info(tmp_path / "initpars.h5", "M")[1] == h5.I64 and h5.info(tmp_path / "initpars.h5", "dt")[1] == h5.F64
+    assert np.array_equal(h5.read(tmp_path / "initdata.3.h5", "phi0"), phi)
+    assert not h5.read(tmp_path / "initdata.3.h5", "bat0").any()
+    h5.write_inputs(tmp_path / "plain", eta, phi, 1.0, 1.0, 1.0, T=1, dtsave=1.0)
+    assert "M" not in h5.read_params(tmp_path / "plain" / "initpars.h5")
