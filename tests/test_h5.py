@@ -198,3 +198,16 @@ def test_run_inputs_round_trip(tmp_path):
     assert not h5.read(tmp_path / "initdata.3.h5", "bat0").any()
     h5.write_inputs(tmp_path / "plain", eta, phi, 1.0, 1.0, 1.0, T=1, dtsave=1.0)
     assert "M" not in h5.read_params(tmp_path / "plain" / "initpars.h5")
+
+
+def test_make_inputs_cli(tmp_path):
+    from hos_b200 import make_inputs
+
+    assert make_inputs.main([str(tmp_path / "j"), "jonswap", "--n", "32", "--lx", "600", "--kp-index", "4",
+                             "--order", "4", "--dt", "0.1", "--T", "2"]) == 0
+    p = h5.read_params(tmp_path / "j" / "initpars.h5")
+    assert (p["Nx"], p["Ny"], p["Lx"], p["M"], p["dt"], p["T"]) == (32, 32, 600.0, 4.0, 0.1, 2.0)
+    eta = h5.read(tmp_path / "j" / "initdata.1.h5", "eta0")
+    assert eta.shape == (32, 32) and abs(eta.mean()) < 1e-12 and eta.std() > 0
+    assert make_inputs.main([str(tmp_path / "s"), "stokes", "--n", "16", "--ny", "8", "--runsubid", "2"]) == 0
+    assert h5.read(tmp_path / "s" / "initdata.2.h5", "phi0").shape == (16, 8)
