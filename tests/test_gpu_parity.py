@@ -70,9 +70,13 @@ def test_stokes_100_rk4_steps_drop_in_gate(golden):
         eta, phi = f.state_physical()
     assert rel(u[0], d["u100"][0]) < TOL_STEPS
     assert rel(u[1], d["u100"][1]) < TOL_STEPS
-    # the parity metric is stated on physical eta and phi_s
-    assert rel(eta, hn.ifft2(d["u100"][0])) < TOL_STEPS
-    assert rel(phi, hn.ifft2(d["u100"][1])) < TOL_STEPS
+    # the parity metric is stated on physical eta and phi_s: max|d|/max|ref| and ||d||_2/||ref||_2
+    eta_ref, phi_ref = hn.ifft2(d["u100"][0]), hn.ifft2(d["u100"][1])
+    assert rel(eta, eta_ref) < TOL_STEPS and rel(phi, phi_ref) < TOL_STEPS
+    assert np.linalg.norm(eta - eta_ref) / np.linalg.norm(eta_ref) < TOL_STEPS
+    assert np.linalg.norm(phi - phi_ref) / np.linalg.norm(phi_ref) < TOL_STEPS
+    # volume (the mean of eta, eta-hat at k = 0) as the reference keeps it
+    assert abs(u[0][0, 0] - d["u100"][0][0, 0]) < 1e-15
     assert abs(t - float(d["t100"])) < 1e-12
     assert len(H) == 100
     assert np.max(np.abs(H - d["ham"])) / np.max(np.abs(d["ham"])) < TOL_STEPS
