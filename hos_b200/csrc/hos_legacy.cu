@@ -194,6 +194,10 @@ void sol_update_RK(double* u, double* t, double dt, char* dtflag) {
     }
   }
   if (hos_clear_history(h) || hos_step(h, dt, 1)) {
+    // the device state may be partly advanced: forget it, so that the next
+    // call uploads the caller's array again instead of syncing this one over it
+    L.resident = nullptr;
+    L.host_stale = false;
     report("sol_update_RK");
     return;
   }

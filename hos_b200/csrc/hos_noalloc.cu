@@ -44,6 +44,7 @@ static __device__ __align__(256) double2 g_noalloc_tw[3 * NOALLOC_MAX_LEN];
 struct DevPtrs {
   double2* spec = nullptr;
   double2* tw = nullptr;
+  unsigned long long ctx_id = 0;  // the context the addresses belong to
   bool ready = false;
 };
 DevPtrs g_dev[NOALLOC_MAX_DEVICES];
@@ -70,12 +71,43 @@ int fail(int code, const char* msg) {
 
 bool pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 
-// One-time set-up per device: the device addresses of the two arrays, taken
-// with the device current.
+// Unique id of the calling thread's current context (driver entry points
+// cuCtxGetCurrent / cuCtxGetId, fetched through the runtime so that the
+// library needs no link against the driver library); 0 if unavailable.
+unsigned long long current_context_id() {
+  typedef int (*GetCurrentFn)(void**);
+  typedef int (*GetIdFn)(void*, unsigned long long*);
+  static GetCurrentFn get_current = nullptr;
+  static GetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetIdFn>(f);
+    (void)cudaGetLastError();
+  });
+  void* c = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&c) != 0 || !c || get_id(c, &id) != 0) return 0;
+  return id;
+}
+
+// Set-up per device: the device addresses of the two arrays, taken with the
+// device current.  It runs on the first call on a device, and again if that
+// device's context has since been replaced (cudaDeviceReset, which reloads
+// the library's device code at new addresses).
 int setup_device(int dev, DevPtrs** out) {
   if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(HOS_ERR_ARG, "device index out of range");
+  const unsigned long long cid = current_context_id();  // 0: no context current on this thread yet
   std::lock_guard<std::mutex> lk(g_mu);
   DevPtrs& d = g_dev[dev];
+  if (d.ready && cid != d.ctx_id) d.ready = false;
   if (!d.ready) {
     cudaError_t e = cudaGetSymbolAddress((void**)&d.spec, g_noalloc_spec);
     if (e == cudaSuccess) e = cudaGetSymbolAddress((void**)&d.tw, g_noalloc_tw);
@@ -83,6 +115,7 @@ int setup_device(int dev, DevPtrs** out) {
       (void)cudaGetLastError();
       return fail(HOS_ERR_CUDA, cudaGetErrorString(e));
     }
+    d.ctx_id = current_context_id();  // the lookup made the device's context current
     d.ready = true;
   }
   *out = &d;

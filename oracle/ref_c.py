@@ -6,6 +6,10 @@ hosm_2d_par.c, operators_par.c, time_schemes_par.c and fft_routines_2d_par.c
 single-rank FFTW-MPI shim and oracle/ref_harness.c (see oracle/Makefile).
 Each library keeps the reference's process-global state, so one RefC object
 per order is live at a time; ``setup`` is re-run when the grid changes.
+
+``dealias="d23"`` selects the build whose operators_par.c has the two
+dealias bounds (operators_par.c:290-291) replaced by floor(Nx/3),
+floor(Ny/3) (the "2/3 rule"; oracle/Makefile makes it for M = 4).
 """
 from __future__ import annotations
 
@@ -21,18 +25,20 @@ _P = ctypes.c_void_p
 _libs = {}
 
 
-def lib_path(M):
-    return os.path.join(_HERE, "_ref", f"libhosref_M{int(M)}.so")
+def lib_path(M, dealias=""):
+    suffix = f"_{dealias}" if dealias else ""
+    return os.path.join(_HERE, "_ref", f"libhosref_M{int(M)}{suffix}.so")
 
 
-def available(M=3):
-    return os.path.exists(lib_path(M))
+def available(M=3, dealias=""):
+    return os.path.exists(lib_path(M, dealias))
 
 
-def _load(M):
-    if M in _libs:
-        return _libs[M]
-    path = lib_path(M)
+def _load(M, dealias=""):
+    key = (M, dealias)
+    if key in _libs:
+        return _libs[key]
+    path = lib_path(M, dealias)
     if not os.path.exists(path):
         raise FileNotFoundError(f"{path} missing: run `make -C oracle` where the reference sources are present")
     lib = ctypes.CDLL(path)
@@ -50,7 +56,7 @@ def _load(M):
     lib.ref_rampfun.argtypes = [_D]
     lib.ref_rampfun.restype = _D
     lib.ref_nlevs.restype = ctypes.c_int
-    _libs[M] = lib
+    _libs[key] = lib
     return lib
 
 
@@ -59,9 +65,10 @@ def _p(a):
 
 
 class RefC:
-    def __init__(self, M, nx, ny, lx=2 * math.pi, ly=2 * math.pi, g=1.0, rampflg=0, tramp=1.0, scheme=2):
+    def __init__(self, M, nx, ny, lx=2 * math.pi, ly=2 * math.pi, g=1.0, rampflg=0, tramp=1.0, scheme=2,
+                 dealias=""):
         self.M = int(M)
-        self.lib = _load(self.M)
+        self.lib = _load(self.M, dealias)
         assert self.lib.ref_nlevs() == self.M - 1
         self.nx, self.ny, self.h = int(nx), int(ny), int(ny) // 2
         self.args = (self.nx, self.ny, float(lx), float(ly), float(g), int(rampflg), float(tramp), int(scheme))

@@ -7,6 +7,10 @@ Run from the repository root after `make -C oracle`:
 
     python tests/golden/make_golden.py
 
+`python tests/golden/make_golden.py large` makes the benchmark-size cases
+alone (512^2 M=4 with both dealias rules, 1024^2 M=5; about ten minutes
+on eight cores).
+
 Every case stores its inputs and the oracle's outputs in one .npz file.  The
 reference ships no test vectors of its own, so these fixtures are the
 pinned record of what the reference code computes on seeded inputs and on
@@ -123,7 +127,7 @@ def shipped_case():
     the modes the dealias mask keeps, and the energy series."""
     from hos_b200 import h5
 
-    src = "/root/reference/Csource/2dpar"
+    from oracle import REFERENCE_SRC as src
     p = h5.read_params(os.path.join(src, "initpars.h5"))
     eta = h5.read(os.path.join(src, "initdata.1.h5"), "eta0")
     phi = h5.read(os.path.join(src, "initdata.1.h5"), "phi0")
@@ -139,8 +143,43 @@ def shipped_case():
          eta_l2=np.linalg.norm(eta), eta_sum=eta.sum())
 
 
+LARGE_CASES = {
+    # name: (n, M, kp, kp*Hs/2, gamma, s, seed, dealias variant)
+    "jonswap512_m4_rk4_100": (512, 4, 16.0, 0.10, 3.3, 15.0, 2, ""),
+    "jonswap512_m4_d23_rk4_100": (512, 4, 16.0, 0.10, 3.3, 15.0, 2, "d23"),
+    "jonswap1024_m5_rk4_100": (1024, 5, 24.0, 0.12, 3.3, 10.0, 1000, ""),
+}
+
+
+def large_case(name, nsteps=100):
+    """A benchmark-size JONSWAP sea run 100 RK4 steps (dt = Tp/50) by the
+    reference's code.  The state of the reference stays inside the dealias
+    mask (the initial state is dealiased and every stage derivative is), so
+    only the kept modes are stored, as (row, column, value), together with a
+    checksum of the seeded initial fields so that a test regenerating them
+    can tell that it got the same inputs."""
+    n, M, kp, st, gamma, spread, seed, variant = LARGE_CASES[name]
+    eta, phi, info = ic.jonswap(n, n, kp=kp, steepness=st, gamma=gamma, spread_s=spread, seed=seed)
+    dt = info["Tp"] / 50
+    ref = RefC(M, n, n, g=1.0, scheme=2, dealias=variant)
+    u0 = ref.init_state(eta, phi)
+    u1, t1, ham = ref.steps(u0, 0.0, dt, nsteps)
+    mx = my = n // 3 if variant == "d23" else None
+    hn = HosNumpy(n, n, 2 * math.pi, 2 * math.pi, 1.0, M, mx=mx, my=my)
+    mask = hn.Dealias(np.ones((n // 2 + 1, n))) != 0
+    assert not np.any(u1[:, ~mask]), "state outside the dealias mask"
+    keep = np.nonzero(mask)
+    save(name, rows=keep[0].astype(np.int16), cols=keep[1].astype(np.int16), u100=u1[:, keep[0], keep[1]],
+         t100=t1, ham=ham, dt=dt, meta=np.array([n, n, M, 2, seed, hn.mx, hn.my]),
+         ic=np.array([kp, st, gamma, spread]), eta_sum=eta.sum(), eta_l2=np.linalg.norm(eta),
+         phi_l2=np.linalg.norm(phi), hs=info["Hs"])
+
+
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "shipped":
         shipped_case()
+    elif len(sys.argv) > 1 and sys.argv[1] == "large":
+        for nm in (sys.argv[2:] or LARGE_CASES):
+            large_case(nm)
     else:
         main()

@@ -19,7 +19,7 @@ import pytest
 
 from hos_b200 import HosError, h5
 
-REF = "/root/reference/Csource/2dpar"
+from oracle import REFERENCE_SRC as REF  # noqa: E402
 shipped = pytest.mark.skipif(not os.path.exists(os.path.join(REF, "initpars.h5")),
                              reason="reference checkout not present")
 
