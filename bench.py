@@ -61,9 +61,11 @@ def parse():
     ap.add_argument("--no-configs", action="store_true")
     ap.add_argument("--ensemble-fields", type=int, default=256)
     ap.add_argument("--ensemble-steps", type=int, default=500)
-    ap.add_argument("--serve-rate", type=float, default=1.2)
+    ap.add_argument("--ensemble-mode", default="persistent", choices=["persistent", "classes"])
+    ap.add_argument("--serve-utilization", type=float, default=0.7)
     ap.add_argument("--serve-duration", type=float, default=20.0)
-    ap.add_argument("--serve-limit", type=float, default=90.0)
+    ap.add_argument("--serve-limit", type=float, default=80.0)
+    ap.add_argument("--serve-nominal-limit", type=float, default=25.0)
     return ap.parse_args()
 
 
@@ -220,20 +222,23 @@ def cpu_reference_rate(args, eta, phi, info, dt, max_seconds):
 
 
 # ------------------------------------------------------------------ ensemble and serving
-def run_ensemble(args, seed=0):
+def run_ensemble(args, rep):
     """256 independent JONSWAP fields (grids 128/256/512 with weights
     0.5/0.3/0.2, M in {3,4,5}, kp*Hs/2 uniform in [0.05, 0.12], kp = n/16,
     half deep water and half finite depth with kp*h uniform in [1, 3]) in
     FP32 compute / FP64 state, 500 RK4 steps each (dt = Tp/50), advanced as
     one ensemble; compared with the same fields advanced one after another
-    in plain FP64."""
+    in plain FP64.  With several GPUs the 256 fields are split over the
+    ranks by estimated work (hos_b200.partition); the time is the slowest
+    rank's."""
     import numpy as np
     import torch
 
     from hos_b200 import HosEnsemble, HosField
+    from hos_b200.partition import Partition, work
     from hos_b200.serve import _dptr, jonswap_device
 
-    rng = np.random.default_rng(seed)
+    rng = np.random.default_rng(0)
     specs = []
     for i in range(args.ensemble_fields):
         n = int(rng.choice([128, 256, 512], p=[0.5, 0.3, 0.2]))
@@ -241,6 +246,9 @@ def run_ensemble(args, seed=0):
         kp = n / 16.0
         depth = None if i % 2 == 0 else float(rng.uniform(1.0, 3.0)) / kp
         specs.append((n, M, kp, float(rng.uniform(0.05, 0.12)), depth, 7000 + i))
+    all_specs = specs
+    part = Partition(all_specs, lambda sp: work(sp[0], sp[1], args.ensemble_steps), rep.rank, rep.world)
+    specs = [sp for _, sp in part.mine]
     fields, dts, hs = [], [], []
     for (n, M, kp, st, depth, sd) in specs:
         eta, phi, tp = jonswap_device(n, kp, st, sd, depth=depth)
@@ -249,23 +257,34 @@ def run_ensemble(args, seed=0):
         fields.append(f)
         dts.append(tp / 50)
         hs.append(2 * st / kp)
-    ens = HosEnsemble(fields, dts)
-    ens.step(3)
-    ens.sync()
-    torch.cuda.synchronize()
-    stream = torch.cuda.ExternalStream(ens.stream)
+    def timed(mode, nsteps):
+        ens = HosEnsemble(fields, dts, mode=mode)
+        ens.step(3)
+        ens.sync()
+        torch.cuda.synchronize()
+        rep.barrier()
+        stream = torch.cuda.ExternalStream(ens.stream)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(stream)
+        ens.step(nsteps)
+        e1.record(stream)
+        ens.sync()
+        wall = time.perf_counter() - t0
+        info = ens.info
+        ens.close()
+        return rep.max(e0.elapsed_time(e1) / 1e3), wall, info
+
+    # the other mode first, on fewer steps, for comparison
+    other = "classes" if args.ensemble_mode == "persistent" else "persistent"
+    n_other = max(10, args.ensemble_steps // 5)
+    el_o, _, info_o = timed(other, n_other)
+    el, wall, info = timed(args.ensemble_mode, args.ensemble_steps)
+    gp1 = sum(n * n for (n, *_r) in all_specs)
+    gp = gp1 * args.ensemble_steps
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    t0 = time.perf_counter()
-    e0.record(stream)
-    ens.step(args.ensemble_steps)
-    e1.record(stream)
-    ens.sync()
-    wall = time.perf_counter() - t0
-    el = e0.elapsed_time(e1) / 1e3
-    gp = sum(n * n for (n, *_r) in specs) * args.ensemble_steps
-    info = ens.info
-    ens.close()
     # sequential plain FP64: each (n, M, depth?) kind timed alone, weighted by the mix
     seq_s = 0.0
     rates = {}
@@ -286,13 +305,14 @@ def run_ensemble(args, seed=0):
             g.close()
         seq_s += rates[key] * args.ensemble_steps
     # accuracy of the FP32 members: four members rerun in FP64
+    seq_s = rep.sum(seq_s)  # all fields one after another on one GPU
     errs = []
-    for i in range(4):
+    for i in range(min(4, len(specs))):
         (n, M, kp, st, depth, sd) = specs[i]
         eta, phi, tp = jonswap_device(n, kp, st, sd, depth=depth)
         g = HosField(n, n, order=M, precision="fp64", depth=depth)
         g._lib.hos_set_state_physical(g._h, _dptr(eta), _dptr(phi), 0.0)
-        g.step(tp / 50, args.ensemble_steps + 3)
+        g.step(tp / 50, 3 + n_other + 3 + args.ensemble_steps)  # every step the two timed ensembles took
         e64, _ = g.state_physical()
         e32, _ = fields[i].state_physical()
         errs.append(float(np.max(np.abs(e32 - e64)) / hs[i]))
@@ -300,37 +320,96 @@ def run_ensemble(args, seed=0):
     for f in fields:
         f.close()
     return {
-        "fields": len(specs),
+        "fields": len(all_specs),
         "steps": args.ensemble_steps,
+        "mode": args.ensemble_mode,
         "size_classes": info["classes"],
         "launches_per_step": info["launches_per_step"],
+        "other_mode": {"mode": other, "steps": n_other, "launches_per_step": info_o["launches_per_step"],
+                       "grid_point_steps_per_s": gp1 * n_other / el_o},
         "seconds": el,
         "grid_point_steps_per_s": gp / el,
         "sequential_fp64_seconds": seq_s,
         "sequential_fp64_grid_point_steps_per_s": gp / seq_s,
         "speedup_vs_sequential_fp64": seq_s / el,
-        "eta_err_over_Hs_max_of_4_fp64_reruns": max(errs),
+        "eta_err_over_Hs_max_of_4_fp64_reruns": rep.max(max(errs) if errs else 0.0),
+        "ranks": rep.world,
+        "rank_work_imbalance": part.imbalance(),
         "wall_seconds": wall,
         "timing": "CUDA events on the ensemble's stream around the step-graph launches",
     }
 
 
+def sequential_fp64_rate(reqs, cache):
+    """Grid-point-steps/s of the requests run one after another in plain
+    FP64 (each (n, M, depth?) kind timed once on 20 steps, weighted by the
+    requests' work)."""
+    import torch
+
+    from hos_b200 import HosField
+    from hos_b200.serve import _dptr, jonswap_device
+
+    work = secs = 0.0
+    for r in reqs:
+        key = (r.n, r.order, r.depth is not None)
+        if key not in cache:
+            eta, phi, tp = jonswap_device(r.n, r.kp_value, r.steepness, r.seed, depth=r.depth)
+            g = HosField(r.n, r.n, order=r.order, precision="fp64", depth=r.depth)
+            g._lib.hos_set_state_physical(g._h, _dptr(eta), _dptr(phi), 0.0)
+            g.step(tp / 50, 3)
+            g.sync()
+            st = torch.cuda.ExternalStream(g.stream)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            g.step(tp / 50, 20)
+            e1.record(st)
+            g.sync()
+            cache[key] = e0.elapsed_time(e1) / 1e3 / 20
+            g.close()
+        work += r.n * r.n * r.steps
+        secs += cache[key] * r.steps
+    return work / secs if secs > 0 else None
+
+
 def run_serving(args, capacity_gps):
+    """The serving configuration: Poisson arrivals of JONSWAP simulations
+    (grid uniform over 64^2..2048^2, M in 3..6, steps uniform in [100, 2000],
+    half finite depth), FP32 compute / FP64 state, admitted by free HBM.
+    Run twice: the nominal stream (200 requests/s for 10 s, about 100x what
+    one B200 can absorb) with a time limit, reporting completions, backlog
+    and the latency of what completed; and a stream at `serve_utilization`
+    of the measured ensemble capacity, where continuous batching keeps up."""
+    import numpy as np
+
     from hos_b200.serve import Server, poisson_requests
 
+    sizes = np.array([64, 128, 256, 512, 1024, 2048], float)
+    mean_work = float(np.mean(sizes**2)) * 1050.0  # E[n^2] * E[steps]
     nominal = poisson_requests(200.0, 10.0, seed=3)
     offered = sum(r.n * r.n * r.steps for r in nominal) / 10.0
-    reqs = poisson_requests(args.serve_rate, args.serve_duration, seed=4)
-    m = Server(chunk=25).run(reqs, realtime=True, time_limit=args.serve_limit)
+    m_nom = Server(keep_results=False).run(nominal, realtime=True, time_limit=args.serve_nominal_limit)
+    rate = args.serve_utilization * capacity_gps / mean_work
+    reqs = poisson_requests(rate, args.serve_duration, seed=4)
+    m = Server(keep_results=False).run(reqs, realtime=True, time_limit=args.serve_limit)
+    done = [r for r in reqs if r.status == "done"]
+    seq = sequential_fp64_rate(done, {}) if done else None
     m.update({
-        "arrival_rate_per_s": args.serve_rate,
+        "arrival_rate_per_s": rate,
         "arrival_window_s": args.serve_duration,
+        "target_utilization": args.serve_utilization,
         "request_mix": "grid uniform over 64^2..2048^2 (powers of two), M in 3..6, steps uniform in [100, 2000], "
                        "half finite depth kp*h in [1,3], FP32 compute / FP64 state",
-        "nominal_stream": {"rate_per_s": 200.0, "window_s": 10.0, "requests": len(nominal),
-                           "offered_grid_point_steps_per_s": offered,
-                           "offered_over_capacity": offered / capacity_gps if capacity_gps else None},
-        "vs_sequential_fp64": None,
+        "sequential_fp64_grid_point_steps_per_s": seq,
+        "vs_sequential_fp64": (m["grid_point_steps_per_s"] / seq) if seq else None,
+        "nominal_stream": {
+            "rate_per_s": 200.0, "window_s": 10.0, "requests": len(nominal), "time_limit_s": args.serve_nominal_limit,
+            "offered_grid_point_steps_per_s": offered,
+            "offered_over_capacity": offered / capacity_gps if capacity_gps else None,
+            "completed": m_nom["completed"], "backlog_queued": m_nom["backlog_queued"],
+            "backlog_running": m_nom["backlog_running"], "p50_s_of_completed": m_nom["p50_s"],
+            "p99_s_of_completed": m_nom["p99_s"], "grid_point_steps_per_s": m_nom["grid_point_steps_per_s"],
+        },
     })
     return m
 
@@ -582,11 +661,9 @@ def run_ours(args, rep):
     if not args.no_configs:
         line["other_configs"] = run_configs(args)
     if not args.no_ensemble:
-        ens = run_ensemble(args, seed=rank)
+        ens = run_ensemble(args, rep)
         line["ensemble"] = ens
-        srv = run_serving(args, ens["grid_point_steps_per_s"])
-        srv["vs_sequential_fp64"] = srv["grid_point_steps_per_s"] / ens["sequential_fp64_grid_point_steps_per_s"]
-        line["serving"] = srv
+        line["serving"] = run_serving(args, ens["grid_point_steps_per_s"])
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
         cb = cpu_reference_rate(args, eta, phi, info, dt, max_seconds=20.0)
@@ -627,8 +704,11 @@ def run_ours(args, rep):
                                                   "speedup_vs_sequential_fp64")}
     if "serving" in line:
         sv = line["serving"]
-        summ["serving"] = {k: sv.get(k) for k in ("completed", "p50_s", "p99_s", "grid_point_steps_per_s",
-                                                  "vs_sequential_fp64")}
+        summ["serving"] = {k: sv.get(k) for k in ("arrival_rate_per_s", "completed", "p50_s", "p99_s",
+                                                  "grid_point_steps_per_s", "vs_sequential_fp64")}
+        nm = sv.get("nominal_stream", {})
+        summ["serving_nominal_200_per_s"] = {k: nm.get(k) for k in ("completed", "backlog_queued", "backlog_running",
+                                                                     "p50_s_of_completed", "p99_s_of_completed")}
     line["summary"] = summ
     for fl in fields.values():
         fl.close()

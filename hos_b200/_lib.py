@@ -106,6 +106,11 @@ _SIGNATURES = {
     "hos_profile_stage": (_I, [_H, _D, _I, ctypes.POINTER(HosPassStat), _I, ctypes.POINTER(_I)]),
     "hos_launches_per_step": (_I, [_H]),
     "hos_ensemble_create": (_I, [ctypes.POINTER(_H), ctypes.POINTER(_D), _I, ctypes.POINTER(_H)]),
+    "hos_ensemble_create_ex": (_I, [ctypes.POINTER(_H), ctypes.POINTER(_D), _I, _I, ctypes.POINTER(_H)]),
+    "hos_ensemble_set_wait_limit": (_I, [_H, ctypes.c_longlong]),
+    "hos_ensemble_set_steps": (_I, [_H, ctypes.POINTER(_I)]),
+    "hos_ensemble_get_remaining": (_I, [_H, ctypes.POINTER(_I)]),
+    "hos_ensemble_withhold_dependency": (_I, [_H, _I]),
     "hos_ensemble_step": (_I, [_H, _I]),
     "hos_ensemble_sync": (_I, [_H]),
     "hos_ensemble_info": (_I, [_H, ctypes.POINTER(_I), ctypes.POINTER(_I)]),

@@ -30,6 +30,7 @@
 #include <vector>
 
 #include "hos_gpu.h"
+#include "hos_persist.h"
 #include "hos_registry.h"
 
 namespace hos {
@@ -84,63 +85,19 @@ __global__ void k_nonfinite(const double2* u, size_t n, int* flag) {
 }
 
 // ---------------------------------------------------------------- step end
-// Sums the stage-0 Hamiltonian partials in a fixed order (one block, fixed
-// strides, fixed tree), records (t, H) and advances t
-// (time_schemes_par.c:73-93,119).
-struct StepEndArgs {
-  const double* ham_part;
-  int nparts;
-  double* tdev;
-  double dt;
-  long long* stepdev;
-  double* ham_hist;
-  double* t_hist;
-  int hist_cap;
-  long long* bad_step;  // first step whose energy was not finite (-1: none)
-  int* any_bad;         // ensemble-wide word set with bad_step (nullptr outside ensembles)
-};
-
-__device__ void step_end_body(const double* ham_part, int nparts, double* tdev, double dt, long long* stepdev,
-                              double* ham_hist, double* t_hist, int hist_cap, long long* bad_step, int* any_bad);
-
+// The step end (StepEndArgs, step_end_body) is in hos_kernels.cuh.
 __global__ void __launch_bounds__(256) k_step_end(const double* ham_part, int nparts, double* tdev, double dt,
                                                   long long* stepdev, double* ham_hist, double* t_hist, int hist_cap,
                                                   long long* bad_step) {
-  step_end_body(ham_part, nparts, tdev, dt, stepdev, ham_hist, t_hist, hist_cap, bad_step, nullptr);
+  pdl_enter();
+  const StepEndArgs a{ham_part, nparts, tdev, dt, stepdev, ham_hist, t_hist, hist_cap, bad_step, nullptr};
+  step_end_body(a, blockDim.x);
 }
 
 // One block per ensemble member.
 __global__ void __launch_bounds__(256) k_step_end_b(const StepEndArgs* __restrict__ arr) {
-  const StepEndArgs& a = arr[blockIdx.x];
-  step_end_body(a.ham_part, a.nparts, a.tdev, a.dt, a.stepdev, a.ham_hist, a.t_hist, a.hist_cap, a.bad_step, a.any_bad);
-}
-
-__device__ void step_end_body(const double* ham_part, int nparts, double* tdev, double dt, long long* stepdev,
-                              double* ham_hist, double* t_hist, int hist_cap, long long* bad_step, int* any_bad) {
   pdl_enter();
-  __shared__ double red[256];
-  double s = 0.0;
-  for (int i = threadIdx.x; i < nparts; i += blockDim.x) s += ham_part[i];
-  red[threadIdx.x] = s;
-  __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
-    __syncthreads();
-  }
-  if (threadIdx.x != 0) return;
-  const long long st = *stepdev;
-  if (st >= 0) {  // ring of hist_cap records
-    ham_hist[st % hist_cap] = red[0];
-    t_hist[st % hist_cap] = *tdev;
-  }
-  // the energy sums every mode of eta and phi, so a NaN or Inf anywhere in the
-  // state shows here; the host reads this word at hos_sync
-  if (!isfinite(red[0])) {
-    if (*bad_step < 0) *bad_step = st;
-    if (any_bad) *any_bad = 1;
-  }
-  *tdev = *tdev + dt;
-  *stepdev = st + 1;
+  step_end_body(arr[blockIdx.x], blockDim.x);
 }
 
 // Elementwise spectral operators on one field [h+1][nx] (operators_par.c):
@@ -510,7 +467,10 @@ int make_cfg(hos_ctx* c, int prec, const ElemChoice& ec, PassCfg* o) {
   const size_t cs = prec ? sizeof(float2) : sizeof(double2);
   const int exi = pick_elems(prec, c->nx, ec.xi), exf = pick_elems(prec, c->nx, ec.xf);
   const int eyi = pick_elems(prec, c->h, ec.yi), eyf = pick_elems(prec, c->h, ec.yf);
-  const int eys = pick_elems(prec, c->h, ec.ys);
+  int eys = pick_elems(prec, c->h, ec.ys);
+  // a 256-thread block of the stage y-inverse at 16 elements per thread
+  // would hold more lines than the grid has rows: use 8 (small grids only)
+  if (eys == 16 && MAX_THREADS / (c->h / 16) > c->nx) eys = pick_elems(prec, c->h, 8);
   for (int m = 0; m < 2; m++) o->xinv[m] = lookup_xinv(prec, m, c->nx, exi);
   for (int m = 0; m < 3; m++) o->xfwd[m] = lookup_xfwd(prec, m, c->nx, exf);
   for (int m = 0; m < 2; m++) o->yinv[m] = lookup_yinv(prec, m, c->h, m == YI_JOBS ? eys : eyi);
@@ -936,7 +896,7 @@ int enqueue_step(hos_ctx* c, double dt) {
     if (rc) return rc;
   }
   const double* hp = c->ham_part;
-  launch_pdl(k_step_end, dim3(1), 256, 0, c->st, hp, xgrid(c, c->cfg.xf), c->tdev, dt, c->stepdev, c->ham_hist,
+  launch_pdl(k_step_end, dim3(1), 256, 0, c->st, hp, c->nparts, c->tdev, dt, c->stepdev, c->ham_hist,
              c->t_hist, (int)HIST_CAP, c->bad_step);
   return HOS_OK;
 }
@@ -1092,6 +1052,14 @@ struct hos_ens {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   int launches_per_step = 0;
+  // persistent mode (HOS_ENS_PERSISTENT): one launch of k_persist per step
+  int mode = 0;
+  PersistArgs pa{};
+  void* pbuf = nullptr;  // counters, task list, item list, argument blob
+  int pblocks = 0;
+  size_t psmem = 0;
+  int ntasks = 0;
+  int withhold = 0;      // test hook: one task waits for an item that never exists
 };
 
 namespace {
@@ -1168,7 +1136,7 @@ int plan_step(hos_ens* E, std::vector<std::vector<BatchLaunch>>& per_class, std:
     std::vector<StepEndArgs> se;
     for (int f : K.idx) {
       hos_ctx* c = E->mem[f];
-      se.push_back(StepEndArgs{c->ham_part, xgrid(c, c->cfg.xf), c->tdev, E->dt[f], c->stepdev, c->ham_hist,
+      se.push_back(StepEndArgs{c->ham_part, c->nparts, c->tdev, E->dt[f], c->stepdev, c->ham_hist,
                                c->t_hist, HIST_CAP, c->bad_step, E->any_bad});
     }
     end_off.push_back(put(se.data(), se.size() * sizeof(StepEndArgs)));
@@ -1239,8 +1207,177 @@ int build_ens_graph(hos_ens* E) {
   return HOS_OK;
 }
 
+// ---------------------------------------------------------------- persistent plan
+// The tasks of one RK step of every member (hos_persist.h): the passes
+// build_stage gives for each stage, re-shaped for PERSIST_THREADS threads,
+// then the step end.  Work items are dealt round by round over the members.
+constexpr int PERSIST_ITEM_CAP = 24;  // work items per task at most (more blocks per item above)
+
+int size_index(int n, int base) {
+  for (int s = 0; s < PERSIST_SIZES; s++)
+    if (n == (base << s)) return s;
+  return -1;
+}
+
+int plan_persist(hos_ens* E) {
+  struct TaskImg {
+    PTask t;
+    size_t arg_off;
+  };
+  std::vector<unsigned char> blob;
+  auto put = [&](const void* p, size_t n) {
+    size_t off = (blob.size() + 255) & ~(size_t)255;
+    blob.resize(off + n);
+    std::memcpy(blob.data() + off, p, n);
+    return off;
+  };
+  const int nm = (int)E->mem.size();
+  std::vector<std::vector<TaskImg>> per(nm);
+  std::vector<long long> member_items(nm, 0);
+  size_t smem = 0;
+  for (int f = 0; f < nm; f++) {
+    hos_ctx* c = E->mem[f];
+    const PassCfg& g = c->cfg;
+    const int sx = size_index(c->nx, 64), sy = size_index(c->h, 32);
+    if (sx < 0 || sy < 0)
+      return fail(HOS_ERR_ARG, "persistent ensemble: member %d grid %dx%d outside 64..2048 x 64..2048", f, c->nx, c->ny);
+    if (g.xi.e != 8 || g.xf.e != 8 || g.yi.e != 8 || g.yf.e != 8 || (g.ys.e != 8 && g.ys.e != 16))
+      return fail(HOS_ERR_ARG, "persistent ensemble: member %d has tuned kernel shapes (default shapes only)", f);
+    const size_t cs = c->prec ? sizeof(float2) : sizeof(double2);
+    long long dep = 0;
+    auto add = [&](int code, int size_idx, int gx, int gy, const void* args, size_t asz, const void* tw0,
+                   const void* tw1) {
+      TaskImg ti{};
+      ti.t.body = code * PERSIST_SIZES + size_idx;
+      ti.t.prec = c->prec;
+      ti.t.member = f;
+      ti.t.gx = gx;
+      ti.t.gy = gy;
+      const int nb = gx * gy;
+      const int items = std::min(nb, PERSIST_ITEM_CAP);
+      ti.t.per_item = (nb + items - 1) / items;
+      ti.t.nitems = (nb + ti.t.per_item - 1) / ti.t.per_item;
+      ti.t.dep = dep;
+      ti.t.tw0 = tw0;
+      ti.t.tw1 = tw1;
+      ti.arg_off = put(args, asz);
+      dep += ti.t.nitems;
+      per[f].push_back(ti);
+    };
+    for (int s = 0; s < c->nst; s++) {
+      std::vector<PassRec> recs;
+      build_stage(c, s, E->dt[f], false, c->u, c->k + (size_t)s * 2 * c->fsz, c->tdev, c->actdev, nullptr, 0, recs);
+      for (PassRec& r : recs) {
+        if (r.kind == L_XINV || r.kind == L_XFWD) {
+          const int P = c->nx / 8;
+          const int lines = PERSIST_THREADS / P;
+          const int gx = (c->h + 1 + lines - 1) / lines;
+          smem = std::max(smem, (size_t)lines * c->nx * cs);
+          if (r.kind == L_XINV)
+            add(PC_XINV_STAGE, sx, gx, r.gy, &r.xi, sizeof(XInvArgs), g.twx, nullptr);
+          else
+            add(r.mode == XF_LEVEL ? PC_XFWD_LEVEL : PC_XFWD_RHS, sx, gx, r.gy, &r.xf, sizeof(XFwdArgs), g.twx,
+                nullptr);
+        } else {
+          const int e = (r.kind == L_YINV && r.mode == YI_JOBS) ? g.ys.e : 8;
+          const int P = c->h / e;
+          const int G = PERSIST_THREADS / P;
+          if (G > c->nx) return fail(HOS_ERR_ARG, "persistent ensemble: member %d grid too small", f);
+          const int phase = (int)(128 / cs);
+          const int target = G >= phase ? 1 : phase / G;
+          int lp = c->h + 1;
+          while (lp % phase != target % phase) lp++;
+          smem = std::max(smem, (size_t)G * lp * cs);
+          if (r.kind == L_YINV) {
+            r.yi.lp = lp;
+            const int code = r.mode == YI_LEVEL ? PC_YINV_LEVEL : (e == 16 ? PC_YINV_JOBS : PC_YINV_JOBS8);
+            add(code, sy, c->nx / G, r.gy, &r.yi, sizeof(YInvArgs), g.twh, g.twy);
+          } else {
+            r.yf.lp = lp;
+            add(r.mode == YF_LEVEL ? PC_YFWD_LEVEL : PC_YFWD_RHS, sy, c->nx / G, r.gy, &r.yf, sizeof(YFwdArgs), g.twh,
+                g.twy);
+          }
+        }
+      }
+    }
+    const StepEndArgs se{c->ham_part, c->nparts, c->tdev, E->dt[f], c->stepdev, c->ham_hist,
+                         c->t_hist, HIST_CAP, c->bad_step, E->any_bad};
+    add(PC_STEP_END, 0, 1, 1, &se, sizeof(se), nullptr, nullptr);
+    member_items[f] = dep;
+  }
+  if (E->withhold && !per.empty() && per[0].size() > 1) per[0][1].t.dep += 1;  // an item that never completes
+
+  // the global list: task k of every member, then task k + 1, ...
+  std::vector<PTask> tasks;
+  std::vector<size_t> arg_off;
+  std::vector<int> item_task;
+  size_t kmax = 0;
+  for (auto& v : per) kmax = std::max(kmax, v.size());
+  for (size_t k = 0; k < kmax; k++)
+    for (int f = 0; f < nm; f++) {
+      if (k >= per[f].size()) continue;
+      PTask t = per[f][k].t;
+      t.first_item = (int)item_task.size();
+      for (int i = 0; i < t.nitems; i++) item_task.push_back((int)tasks.size());
+      tasks.push_back(t);
+      arg_off.push_back(per[f][k].arg_off);
+    }
+  if (item_task.size() > (size_t)0x7fffffff) return fail(HOS_ERR_ARG, "persistent ensemble: too many work items");
+
+  // one device buffer: counters | done[nm] | member_items[nm] | remaining[nm] | tasks | item_task | argument blob
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const size_t o_cnt = 0, o_done = 256, o_mi = al(o_done + nm * 8), o_rem = al(o_mi + nm * 8);
+  const size_t o_tasks = al(o_rem + nm * 4);
+  const size_t o_items = al(o_tasks + tasks.size() * sizeof(PTask));
+  const size_t o_blob = al(o_items + item_task.size() * sizeof(int));
+  const size_t total = o_blob + blob.size();
+  if (E->pbuf) cudaFree(E->pbuf);
+  E->pbuf = nullptr;
+  int rc = dalloc(&E->pbuf, total);
+  if (rc) return rc;
+  char* base = static_cast<char*>(E->pbuf);
+  for (size_t i = 0; i < tasks.size(); i++) tasks[i].args = base + o_blob + arg_off[i];
+  std::vector<unsigned char> img(o_blob, 0);
+  std::memcpy(img.data() + o_mi, member_items.data(), nm * 8);
+  std::memset(img.data() + o_rem, 0xff, nm * 4);  // -1: no step budget
+  std::memcpy(img.data() + o_tasks, tasks.data(), tasks.size() * sizeof(PTask));
+  std::memcpy(img.data() + o_items, item_task.data(), item_task.size() * sizeof(int));
+  HOS_CK(cudaMemcpy(base, img.data(), img.size(), cudaMemcpyHostToDevice));
+  HOS_CK(cudaMemcpy(base + o_blob, blob.data(), blob.size(), cudaMemcpyHostToDevice));
+
+  PersistArgs& a = E->pa;
+  a.tasks = reinterpret_cast<const PTask*>(base + o_tasks);
+  a.item_task = reinterpret_cast<const int*>(base + o_items);
+  a.nitems = (int)item_task.size();
+  a.done = reinterpret_cast<unsigned long long*>(base + o_done);
+  a.member_items = reinterpret_cast<const long long*>(base + o_mi);
+  a.nmembers = nm;
+  a.remaining = reinterpret_cast<int*>(base + o_rem);
+  a.head = reinterpret_cast<unsigned int*>(base + o_cnt);
+  a.finished = reinterpret_cast<unsigned int*>(base + o_cnt + 4);
+  a.epoch = reinterpret_cast<unsigned long long*>(base + o_cnt + 8);
+  a.err = reinterpret_cast<int*>(base + o_cnt + 16);
+  a.err_info = reinterpret_cast<long long*>(base + o_cnt + 32);
+  if (a.wait_limit_ns <= 0) a.wait_limit_ns = 2000000000LL;  // 2 s
+  E->ntasks = (int)tasks.size();
+
+  // resident blocks: the launch is cooperative, so all of them must fit at once
+  smem = std::max(smem, (size_t)16);
+  HOS_CK(persist_set_smem(smem));
+  int per_sm = 0;
+  HOS_CK(persist_occupancy(&per_sm, smem));
+  int sms = 0;
+  HOS_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, E->mem[0]->device));
+  if (per_sm < 1) return fail(HOS_ERR_ARG, "persistent ensemble: kernel does not fit an SM");
+  E->pblocks = per_sm * sms;
+  E->psmem = smem;
+  E->launches_per_step = 1;
+  return HOS_OK;
+}
+
 void release_ens(hos_ens* E) {
   if (!E) return;
+  if (E->pbuf) cudaFree(E->pbuf);
   if (E->gexec) cudaGraphExecDestroy(E->gexec);
   if (E->graph) cudaGraphDestroy(E->graph);
   if (E->dargs) cudaFree(E->dargs);
@@ -1406,7 +1543,7 @@ int hos_create(const hos_params* p, hos_handle* out) {
     release(c);
     return rc;
   }
-  c->nparts = xgrid(c, c->cfg.xf);
+  c->nparts = c->h + 1;  // one Hamiltonian partial per ky row
   rc = dalloc(&c->ham_part, (size_t)c->nparts * sizeof(double));
   if (rc) {
     release(c);
@@ -1756,9 +1893,15 @@ int hos_hamiltonian(hos_handle h, const double* eta, const double* eta_t, const 
 }
 
 int hos_ensemble_create(const hos_handle* members, const double* dt, int n, hos_ensemble* out) {
+  return hos_ensemble_create_ex(members, dt, n, HOS_ENS_CLASSES, out);
+}
+
+int hos_ensemble_create_ex(const hos_handle* members, const double* dt, int n, int mode, hos_ensemble* out) {
   if (!members || !dt || !out || n < 1) return fail(HOS_ERR_ARG, "bad argument");
+  if (mode != HOS_ENS_CLASSES && mode != HOS_ENS_PERSISTENT) return fail(HOS_ERR_ARG, "unknown ensemble mode %d", mode);
   *out = nullptr;
   hos_ens* E = new hos_ens();
+  E->mode = mode;
   for (int i = 0; i < n; i++) {
     if (!members[i]) {
       delete E;
@@ -1807,7 +1950,20 @@ int hos_ensemble_create(const hos_handle* members, const double* dt, int n, hos_
     release_ens(E);
     return rc;
   }
-  rc = build_ens_graph(E);
+  if (E->mode == HOS_ENS_PERSISTENT) {
+    for (size_t i = 1; i < E->mem.size(); i++)
+      if (E->mem[i]->device != E->mem[0]->device) {
+        release_ens(E);
+        return fail(HOS_ERR_ARG, "persistent ensemble: members on different devices");
+      }
+    int dev0 = 0;
+    cudaGetDevice(&dev0);
+    cudaSetDevice(E->mem[0]->device);
+    rc = plan_persist(E);
+    cudaSetDevice(dev0);
+  } else {
+    rc = build_ens_graph(E);
+  }
   if (rc) {
     release_ens(E);
     return rc;
@@ -1818,14 +1974,61 @@ int hos_ensemble_create(const hos_handle* members, const double* dt, int n, hos_
 
 int hos_ensemble_step(hos_ensemble e, int nsteps) {
   if (!e || nsteps < 0) return fail(HOS_ERR_ARG, "bad argument");
+  if (e->mode == HOS_ENS_PERSISTENT) {
+    for (int i = 0; i < nsteps; i++) HOS_CK(persist_launch(e->pa, e->pblocks, e->psmem, e->st));
+    return HOS_OK;
+  }
   for (int i = 0; i < nsteps; i++) HOS_CK(cudaGraphLaunch(e->gexec, e->st));
   return HOS_OK;
+}
+
+int hos_ensemble_set_wait_limit(hos_ensemble e, long long ns) {
+  if (!e || ns <= 0) return fail(HOS_ERR_ARG, "bad argument");
+  e->pa.wait_limit_ns = ns;
+  return HOS_OK;
+}
+
+int hos_ensemble_set_steps(hos_ensemble e, const int* steps) {
+  if (!e || !steps) return fail(HOS_ERR_ARG, "null argument");
+  if (e->mode != HOS_ENS_PERSISTENT) return fail(HOS_ERR_STATE, "step budgets need a persistent ensemble");
+  HOS_CK(cudaMemcpyAsync(e->pa.remaining, steps, e->mem.size() * sizeof(int), cudaMemcpyHostToDevice, e->st));
+  HOS_CK(cudaStreamSynchronize(e->st));
+  return HOS_OK;
+}
+
+int hos_ensemble_get_remaining(hos_ensemble e, int* steps) {
+  if (!e || !steps) return fail(HOS_ERR_ARG, "null argument");
+  if (e->mode != HOS_ENS_PERSISTENT) return fail(HOS_ERR_STATE, "step budgets need a persistent ensemble");
+  HOS_CK(cudaMemcpyAsync(steps, e->pa.remaining, e->mem.size() * sizeof(int), cudaMemcpyDeviceToHost, e->st));
+  HOS_CK(cudaStreamSynchronize(e->st));
+  return HOS_OK;
+}
+
+int hos_ensemble_withhold_dependency(hos_ensemble e, int on) {
+  if (!e) return fail(HOS_ERR_ARG, "null ensemble");
+  if (e->mode != HOS_ENS_PERSISTENT) return fail(HOS_ERR_STATE, "only persistent ensembles have work lists");
+  HOS_CK(cudaStreamSynchronize(e->st));
+  e->withhold = on ? 1 : 0;
+  return plan_persist(e);
 }
 
 int hos_ensemble_sync(hos_ensemble e) {
   if (!e) return fail(HOS_ERR_ARG, "null ensemble");
   HOS_CK(cudaStreamSynchronize(e->st));
   HOS_CK(cudaGetLastError());
+  if (e->mode == HOS_ENS_PERSISTENT) {
+    int err = 0;
+    HOS_CK(cudaMemcpy(&err, e->pa.err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) {
+      long long info[4] = {0, 0, 0, 0};
+      HOS_CK(cudaMemcpy(info, e->pa.err_info, sizeof(info), cudaMemcpyDeviceToHost));
+      HOS_CK(cudaMemset(e->pa.err, 0, sizeof(int)));
+      return fail(HOS_ERR_TIMEOUT,
+                  "persistent ensemble: item %lld of member %lld waited past the limit for %lld completed items "
+                  "(saw %lld); the members' states are not valid until set again",
+                  info[0], info[1], info[2], info[3]);
+    }
+  }
   int bad = 0;
   HOS_CK(cudaMemcpy(&bad, e->any_bad, sizeof(int), cudaMemcpyDeviceToHost));
   if (bad) return fail(HOS_ERR_NONFINITE, "a member's state became non-finite (hos_health on each member tells which)");
@@ -1836,7 +2039,7 @@ void* hos_ensemble_stream(hos_ensemble e) { return e ? (void*)e->st : nullptr; }
 
 int hos_ensemble_info(hos_ensemble e, int* nclasses, int* launches_per_step) {
   if (!e) return fail(HOS_ERR_ARG, "null ensemble");
-  if (nclasses) *nclasses = (int)e->cls.size();
+  if (nclasses) *nclasses = e->mode == HOS_ENS_PERSISTENT ? 1 : (int)e->cls.size();
   if (launches_per_step) *launches_per_step = e->launches_per_step;
   return HOS_OK;
 }

@@ -138,27 +138,28 @@ struct XInvArgs {
 // STAGE outputs (blockIdx.y = o): 0 eta, 1 i kx eta, 2 phi, 3 i kx phi,
 // 3+p d_z^p phi (p >= 1).  The stage input u + sum coef*k is formed on the
 // fly (time_schemes_par.c:38-67).
-template <typename T, int NX, int E, int MODE, bool B>
-__global__ void __launch_bounds__(MAX_THREADS, 2) k_xinv(const __grid_constant__ XInvArgs a0,
-                                                         const XInvArgs* __restrict__ arr, const void* twv) {
-  pdl_enter();
-  const XInvArgs& a = B ? arr[blockIdx.z] : a0;  // batched: one field per z
-  if (B && (int)blockIdx.y >= a.ycount) return;
+// Pass bodies.  Every pass is written as a device function of the block's
+// coordinates (bx, by) and its thread count, so that the same code runs as a
+// kernel of its own (the wrappers below pass blockIdx and blockDim) and as a
+// work item of the persistent ensemble kernel (hos_persist.cu), which gives
+// each item a virtual block.  smraw is the block's dynamic shared memory.
+template <typename T, int NX, int E, int MODE>
+__device__ __forceinline__ void xinv_body(const XInvArgs& a, int bx, int by, int nthreads, const void* twv,
+                                          unsigned char* smraw) {
   using C = cpx<T>;
   constexpr int P = NX / E;
   const C* tw = reinterpret_cast<const C*>(twv);
-  extern __shared__ __align__(16) unsigned char smraw[];
   const int line = threadIdx.x / P;
   const int t = threadIdx.x - line * P;
   C* sm = reinterpret_cast<C*>(smraw) + line * line_smem_elems<NX, E>();
-  const int lines = blockDim.x / P;
-  const int row = blockIdx.x * lines + line;
+  const int lines = nthreads / P;
+  const int row = bx * lines + line;
   const int rows = a.rows_dev ? *a.rows_dev : a.rows;
   const Geo& geo = a.geo;
   const size_t fsz = (size_t)(geo.h + 1) * NX;
-  const int o = blockIdx.y;
+  const int o = by;
 
-  if (MODE == XI_STAGE && a.set_ramp && blockIdx.x == 0 && o == 0 && threadIdx.x == 0) {
+  if (MODE == XI_STAGE && a.set_ramp && bx == 0 && o == 0 && threadIdx.x == 0) {
     double r = 1.0;
     if (a.rampflg == 1) {
       const double tt = *a.tdev;
@@ -166,7 +167,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_xinv(const __grid_constant__
     }
     *a.rdev = r;
   }
-  if ((int)(blockIdx.x * lines) >= rows) return;  // whole block beyond the active rows
+  if (bx * lines >= rows) return;  // whole block beyond the active rows
   const bool live = row < rows;
   const size_t roff = (size_t)(live ? row : 0) * NX;
   C* z = reinterpret_cast<C*>(a.z) + (size_t)o * fsz;
@@ -209,6 +210,16 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_xinv(const __grid_constant__
   }
 }
 
+template <typename T, int NX, int E, int MODE, bool B>
+__global__ void __launch_bounds__(MAX_THREADS, 2) k_xinv(const __grid_constant__ XInvArgs a0,
+                                                         const XInvArgs* __restrict__ arr, const void* twv) {
+  pdl_enter();
+  const XInvArgs& a = B ? arr[blockIdx.z] : a0;  // batched: one field per z
+  if (B && (int)blockIdx.y >= a.ycount) return;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  xinv_body<T, NX, E, MODE>(a, blockIdx.x, blockIdx.y, blockDim.x, twv, smraw);
+}
+
 // ---------------------------------------------------------------- x forward
 struct XFwdArgs {
   Geo geo;
@@ -233,28 +244,24 @@ struct XFwdArgs {
   double2* kout;                  // this stage's derivative [2][h+1][nx]
   const double* rdev;             // ramp factor
   int ham;                        // accumulate the stage-0 Hamiltonian
-  double* ham_part;               // one partial per block of the eta half
+  double* ham_part;               // one partial per ky row (h+1 of them)
   int final_update;               // u += sum cfin[s] * k_s (time_schemes_par.c:98-116)
   const double2* kall[MAX_STAGES];
   double cfin[MAX_STAGES];
   int nstage;                     // number of stages; k of the last one is in registers
 };
 
-template <typename T, int NX, int E, int MODE, bool B>
-__global__ void __launch_bounds__(MAX_THREADS, 2) k_xfwd(const __grid_constant__ XFwdArgs a0,
-                                                         const XFwdArgs* __restrict__ arr, const void* twv) {
-  pdl_enter();
-  const XFwdArgs& a = B ? arr[blockIdx.z] : a0;
-  if (B && (int)blockIdx.y >= a.ycount) return;
+template <typename T, int NX, int E, int MODE>
+__device__ __forceinline__ void xfwd_body(const XFwdArgs& a, int bx, int by, int nthreads, const void* twv,
+                                          unsigned char* smraw) {
   using C = cpx<T>;
   constexpr int P = NX / E;
   const C* tw = reinterpret_cast<const C*>(twv);
-  extern __shared__ __align__(16) unsigned char smraw[];
   const int line = threadIdx.x / P;
   const int t = threadIdx.x - line * P;
   C* sm = reinterpret_cast<C*>(smraw) + line * line_smem_elems<NX, E>();
-  const int lines = blockDim.x / P;
-  const int row = blockIdx.x * lines + line;
+  const int lines = nthreads / P;
+  const int row = bx * lines + line;
   const Geo& geo = a.geo;
   const size_t fsz = (size_t)(geo.h + 1) * NX;
 
@@ -262,7 +269,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_xfwd(const __grid_constant__
     const T sc = (T)geo.inv_nxny;
     const bool live = row < a.rows;
     const size_t roff = (size_t)(live ? row : 0) * NX;
-    const C* vin = reinterpret_cast<const C*>(a.vin0) + (MODE == XF_PLAIN ? (size_t)blockIdx.y * fsz : 0);
+    const C* vin = reinterpret_cast<const C*>(a.vin0) + (MODE == XF_PLAIN ? (size_t)by * fsz : 0);
     C v[E];
 #pragma unroll
     for (int e = 0; e < E; e++) v[e] = live ? vin[roff + t + e * P] : mkc((T)0, (T)0);
@@ -271,8 +278,8 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_xfwd(const __grid_constant__
     for (int e = 0; e < E; e++) v[e] = cscale(v[e], sc);  // fft_2d's 1/Nx/Ny (exact: powers of two)
     if (MODE == XF_PLAIN) {
       if (live) {
-        double2* out = a.out_spec + (size_t)blockIdx.y * fsz;
-        const bool addk = (a.addk_mask >> blockIdx.y) & 1;
+        double2* out = a.out_spec + (size_t)by * fsz;
+        const bool addk = (a.addk_mask >> by) & 1;
         const double ky = ky_of(geo, row);
 #pragma unroll
         for (int e = 0; e < E; e++) {
@@ -292,9 +299,9 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_xfwd(const __grid_constant__
       return;
     }
     // LEVEL: v holds phi^(n+1) hat; this block emits its z-derivatives of
-    // orders p0+1 .. p0+opb, p0 = blockIdx.y*opb (the forward transform is
+    // orders p0+1 .. p0+opb, p0 = by*opb (the forward transform is
     // repeated per block, so opb trades repeated work for parallel blocks)
-    const int p0 = blockIdx.y * a.opb;
+    const int p0 = by * a.opb;
     const int p1 = min(p0 + a.opb, a.ndz);
     for (int p = p0 + 1; p <= p1; p++) {
       C w[E];
@@ -311,15 +318,15 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_xfwd(const __grid_constant__
   }
 
   // ---- RHS: end of an RK stage (rhs_hos tail, hosm_2d_par.c:181-233, and
-  // sol_update_RK bookkeeping, time_schemes_par.c:70-116).  blockIdx.y = 0
-  // finishes eta_t (and the Hamiltonian), blockIdx.y = 1 finishes phi_t.
+  // sol_update_RK bookkeeping, time_schemes_par.c:70-116).  by = 0
+  // finishes eta_t (and the Hamiltonian), by = 1 finishes phi_t.
   __shared__ double red[MAX_THREADS / 32];
-  const int f = blockIdx.y;
+  const int f = by;
   const int rows = a.rows_dev ? *a.rows_dev : a.rows;
   const bool live = row < rows;
   const bool fft_row = row < a.rows_fft;
   const size_t roff = (size_t)(live ? row : 0) * NX;
-  const bool block_fft = (int)(blockIdx.x * lines) < a.rows_fft;
+  const bool block_fft = bx * lines < a.rows_fft;
   C v[E];
   if (block_fft) {
     const C* vin = reinterpret_cast<const C*>(f == 0 ? a.vin0 : a.vin1);
@@ -373,16 +380,33 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_xfwd(const __grid_constant__
     }
   }
   if (f == 0 && a.ham) {
-    // deterministic block reduction
-    for (int off = 16; off > 0; off >>= 1) hacc += __shfl_down_sync(0xffffffffu, hacc, off);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = hacc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double s = 0.0;
-      for (int wi = 0; wi < (int)(blockDim.x + 31) / 32; wi++) s += red[wi];
-      a.ham_part[blockIdx.x] = s;
+    // one partial per ky row, summed over the row's P threads by a fixed
+    // tree, so that the partials (and the energy the step end forms from
+    // them) do not depend on how many rows a block holds
+    if (P <= 32) {
+      for (int off = P / 2; off > 0; off >>= 1) hacc += __shfl_down_sync(0xffffffffu, hacc, off, P);
+      if (t == 0 && row <= geo.h) a.ham_part[row] = hacc;
+    } else {
+      for (int off = 16; off > 0; off >>= 1) hacc += __shfl_down_sync(0xffffffffu, hacc, off);
+      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = hacc;
+      __syncthreads();
+      if (t == 0 && row <= geo.h) {
+        double s = 0.0;
+        for (int wi = 0; wi < P / 32; wi++) s += red[(threadIdx.x >> 5) + wi];
+        a.ham_part[row] = s;
+      }
     }
   }
+}
+
+template <typename T, int NX, int E, int MODE, bool B>
+__global__ void __launch_bounds__(MAX_THREADS, 2) k_xfwd(const __grid_constant__ XFwdArgs a0,
+                                                         const XFwdArgs* __restrict__ arr, const void* twv) {
+  pdl_enter();
+  const XFwdArgs& a = B ? arr[blockIdx.z] : a0;
+  if (B && (int)blockIdx.y >= a.ycount) return;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  xfwd_body<T, NX, E, MODE>(a, blockIdx.x, blockIdx.y, blockDim.x, twv, smraw);
 }
 
 // Forward y-transform of the values v (pairs of physical points of this
@@ -392,7 +416,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_xfwd(const __grid_constant__
 template <typename T, int H, int E>
 __device__ __forceinline__ void yfwd_finish(cpx<T> (&v)[E], cpx<T>* sm, cpx<T>* tl, int t, int G, int lp,
                                             const cpx<T>* tw, const cpx<T>* twy, cpx<T>* vo, int nx, int ix0,
-                                            int rows_out) {
+                                            int rows_out, int nthreads) {
   using C = cpx<T>;
   constexpr int P = H / E;
   line_fft<T, H, E, false>(v, tl, t, tw);
@@ -429,7 +453,7 @@ __device__ __forceinline__ void yfwd_finish(cpx<T> (&v)[E], cpx<T>* sm, cpx<T>* 
   __syncthreads();
   const int ntot = G * rows_out;
   const int lg = __ffs(G) - 1;  // G is a power of two
-  for (int q = threadIdx.x; q < ntot; q += blockDim.x) {
+  for (int q = threadIdx.x; q < ntot; q += nthreads) {
     const int ky = q >> lg, g = q & (G - 1);
     vo[(size_t)ky * nx + ix0 + g] = sm[(size_t)g * lp + (ky)];
   }
@@ -488,19 +512,14 @@ struct YInvArgs {
   int store_job0;  // 0 when the fused job-0 result has no other reader
 };
 
-template <typename T, int H, int E, int MODE, bool B>
-__global__ void __launch_bounds__(MAX_THREADS, 2) k_yinv(const __grid_constant__ YInvArgs a0,
-                                                         const YInvArgs* __restrict__ arr, const void* twv,
-                                                         const void* twyv) {
-  pdl_enter();
-  const YInvArgs& a = B ? arr[blockIdx.z] : a0;
-  if (B && (int)blockIdx.y >= a.ycount) return;
+template <typename T, int H, int E, int MODE>
+__device__ __forceinline__ void yinv_body(const YInvArgs& a, int bx, int by, int nthreads, const void* twv,
+                                          const void* twyv, unsigned char* smraw) {
   using C = cpx<T>;
   constexpr int P = H / E;
   const C* tw = reinterpret_cast<const C*>(twv);    // length H
   const C* twy = reinterpret_cast<const C*>(twyv);  // length 2H
-  extern __shared__ __align__(16) unsigned char smraw[];
-  const int G = blockDim.x / P;
+  const int G = nthreads / P;
   const int line = threadIdx.x / P;
   const int t = threadIdx.x - line * P;
   C* sm = reinterpret_cast<C*>(smraw);
@@ -508,11 +527,11 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yinv(const __grid_constant__
   const Geo& geo = a.geo;
   const int nx = geo.nx;
   const int ny = 2 * H;
-  const int ix0 = blockIdx.x * G;
+  const int ix0 = bx * G;
   const int ix = ix0 + line;
   const size_t fsz = (size_t)(H + 1) * nx;
   const size_t psz = (size_t)nx * ny;
-  const YJob J = a.jobs[blockIdx.y];
+  const YJob J = a.jobs[by];
   T* pall = reinterpret_cast<T*>(a.phys);
 
   {  // column strip -> line regions; every row's copy is in flight at once
@@ -520,7 +539,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yinv(const __grid_constant__
     const int nin = G * (a.rows_dev ? *a.rows_dev : a.rows_in);
     const int ntot = G * (H + 1);
     const int lg = __ffs(G) - 1;  // G is a power of two
-    for (int q = threadIdx.x; q < ntot; q += blockDim.x) {
+    for (int q = threadIdx.x; q < ntot; q += nthreads) {
       const int ky = q >> lg, g = q & (G - 1);
       const bool live = q < nin;
       cp_async_elem(&sm[(size_t)g * a.lp + ky], live ? zs + (size_t)ky * nx + ix0 + g : zs, live);
@@ -554,11 +573,11 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yinv(const __grid_constant__
   line_fft<T, H, E, true>(v, tl, t, tw);  // starts with a barrier before reusing tl
   // v[e] holds (x[2m], x[2m+1]) for m = t + e*P of physical row ix
   C* po = reinterpret_cast<C*>(pall + (size_t)J.out * psz + (size_t)ix * ny);
-  if (MODE != YI_LEVEL || blockIdx.y != 0 || a.store_job0) {
+  if (MODE != YI_LEVEL || by != 0 || a.store_job0) {
 #pragma unroll
     for (int e = 0; e < E; e++) po[t + e * P] = v[e];
   }
-  if (MODE == YI_LEVEL && blockIdx.y == 0) {
+  if (MODE == YI_LEVEL && by == 0) {
     // W_n = own + sum_{p=1..w_terms} d_p eta^p/p! with own = d_z phi^(n+1)
     // (this block's result) and w_in[q] the field of power q+1; then, when
     // fused, P_(n+1) = -(own eta + sum_{p=2..nx_terms} d'_p eta^p/p!).  Both
@@ -615,8 +634,19 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yinv(const __grid_constant__
       for (int e = 0; e < E; e++) v[e] = mkc(-acc[e].x * et[e].x, -acc[e].y * et[e].y);
     }
   }
-  if (MODE == YI_LEVEL && a.fuse_next && blockIdx.y == 0)
-    yfwd_finish<T, H, E>(v, sm, tl, t, G, a.lp, tw, twy, reinterpret_cast<C*>(a.vout), nx, ix0, H + 1);
+  if (MODE == YI_LEVEL && a.fuse_next && by == 0)
+    yfwd_finish<T, H, E>(v, sm, tl, t, G, a.lp, tw, twy, reinterpret_cast<C*>(a.vout), nx, ix0, H + 1, nthreads);
+}
+
+template <typename T, int H, int E, int MODE, bool B>
+__global__ void __launch_bounds__(MAX_THREADS, 2) k_yinv(const __grid_constant__ YInvArgs a0,
+                                                         const YInvArgs* __restrict__ arr, const void* twv,
+                                                         const void* twyv) {
+  pdl_enter();
+  const YInvArgs& a = B ? arr[blockIdx.z] : a0;
+  if (B && (int)blockIdx.y >= a.ycount) return;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  yinv_body<T, H, E, MODE>(a, blockIdx.x, blockIdx.y, blockDim.x, twv, twyv, smraw);
 }
 
 struct YFwdArgs {
@@ -679,19 +709,14 @@ __device__ __forceinline__ T rhs_point(const YFwdArgs& a, const T* W, T ex, T ey
   return (T)0.5 * (w2m + grad2 * w2m2) - (T)0.5 * (px * px + py * py);  // hosm_2d_par.c:181-206
 }
 
-template <typename T, int H, int E, int MODE, bool B>
-__global__ void __launch_bounds__(MAX_THREADS, 2) k_yfwd(const __grid_constant__ YFwdArgs a0,
-                                                         const YFwdArgs* __restrict__ arr, const void* twv,
-                                                         const void* twyv) {
-  pdl_enter();
-  const YFwdArgs& a = B ? arr[blockIdx.z] : a0;
-  if (B && (int)blockIdx.y >= a.ycount) return;
+template <typename T, int H, int E, int MODE>
+__device__ __forceinline__ void yfwd_body(const YFwdArgs& a, int bx, int by, int nthreads, const void* twv,
+                                          const void* twyv, unsigned char* smraw) {
   using C = cpx<T>;
   constexpr int P = H / E;
   const C* tw = reinterpret_cast<const C*>(twv);
   const C* twy = reinterpret_cast<const C*>(twyv);
-  extern __shared__ __align__(16) unsigned char smraw[];
-  const int G = blockDim.x / P;
+  const int G = nthreads / P;
   const int line = threadIdx.x / P;
   const int t = threadIdx.x - line * P;
   C* sm = reinterpret_cast<C*>(smraw);
@@ -699,7 +724,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yfwd(const __grid_constant__
   const Geo& geo = a.geo;
   const int nx = geo.nx;
   const int ny = 2 * H;
-  const int ix0 = blockIdx.x * G;
+  const int ix0 = bx * G;
   const int ix = ix0 + line;
   const size_t fsz = (size_t)(H + 1) * nx;
   const size_t psz = (size_t)nx * ny;
@@ -737,7 +762,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yfwd(const __grid_constant__
 #pragma unroll
     for (int e = 0; e < E; e++) v[e] = mkc(-v[e].x * et[e].x, -v[e].y * et[e].y);
   } else {
-    const int which = blockIdx.y + a.which_base;
+    const int which = by + a.which_base;
     const C* pex = reinterpret_cast<const C*>(pall + (size_t)a.ex * psz + rowoff);
     const C* pey = reinterpret_cast<const C*>(pall + (size_t)a.ey * psz + rowoff);
     const C* ppx = reinterpret_cast<const C*>(pall + (size_t)a.px * psz + rowoff);
@@ -759,8 +784,63 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yfwd(const __grid_constant__
     }
   }
 
-  yfwd_finish<T, H, E>(v, sm, tl, t, G, a.lp, tw, twy, reinterpret_cast<C*>(a.vout) + (size_t)blockIdx.y * fsz, nx,
-                       ix0, a.rows_out);
+  yfwd_finish<T, H, E>(v, sm, tl, t, G, a.lp, tw, twy, reinterpret_cast<C*>(a.vout) + (size_t)by * fsz, nx, ix0,
+                       a.rows_out, nthreads);
+}
+
+template <typename T, int H, int E, int MODE, bool B>
+__global__ void __launch_bounds__(MAX_THREADS, 2) k_yfwd(const __grid_constant__ YFwdArgs a0,
+                                                         const YFwdArgs* __restrict__ arr, const void* twv,
+                                                         const void* twyv) {
+  pdl_enter();
+  const YFwdArgs& a = B ? arr[blockIdx.z] : a0;
+  if (B && (int)blockIdx.y >= a.ycount) return;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  yfwd_body<T, H, E, MODE>(a, blockIdx.x, blockIdx.y, blockDim.x, twv, twyv, smraw);
+}
+
+// ---------------------------------------------------------------- step end
+// Sums the stage-0 Hamiltonian partials (one per ky row) in a fixed order
+// (fixed strides, fixed tree), records (t, H) and advances t
+// (time_schemes_par.c:73-93,119).  One block of nthreads (a power of two,
+// at most 256) threads.
+struct StepEndArgs {
+  const double* ham_part;
+  int nparts;
+  double* tdev;
+  double dt;
+  long long* stepdev;
+  double* ham_hist;
+  double* t_hist;
+  int hist_cap;
+  long long* bad_step;  // first step whose energy was not finite (-1: none)
+  int* any_bad;         // ensemble-wide word set with bad_step (nullptr outside ensembles)
+};
+
+__device__ __forceinline__ void step_end_body(const StepEndArgs& a, int nthreads) {
+  __shared__ double red[256];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < a.nparts; i += nthreads) s += a.ham_part[i];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = nthreads / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  const long long st = *a.stepdev;
+  if (st >= 0) {  // ring of hist_cap records
+    a.ham_hist[st % a.hist_cap] = red[0];
+    a.t_hist[st % a.hist_cap] = *a.tdev;
+  }
+  // the energy sums every mode of eta and phi, so a NaN or Inf anywhere in the
+  // state shows here; the host reads this word at hos_sync
+  if (!isfinite(red[0])) {
+    if (*a.bad_step < 0) *a.bad_step = st;
+    if (a.any_bad) *a.any_bad = 1;
+  }
+  *a.tdev = *a.tdev + a.dt;
+  *a.stepdev = st + 1;
 }
 
 }  // namespace hos

@@ -9,10 +9,12 @@ number of RK4 steps).  The server
   request that does not fit does not block smaller ones behind it;
 * keeps each admitted field's FP64 spectral state resident on the device
   (one ``HosField`` per request) until it finishes;
-* advances all active fields together as one ``HosEnsemble`` (one launch
-  per pass per size class, one CUDA graph per step) in chunks of at most
-  ``chunk`` steps; requests that arrive meanwhile join at the next chunk
-  boundary, and finished ones leave (their slot and memory are freed);
+* advances all active fields together as one persistent ``HosEnsemble``
+  (one kernel launch per RK step for every member, each member with its own
+  step budget on the device) in chunks of about ``chunk_seconds``; requests
+  that arrive meanwhile are admitted while the chunk runs and join at its
+  end, and a request stops at exactly its own number of steps, inside a
+  chunk, and leaves at the chunk's end (its slot and memory are freed);
 * records for each request its arrival, admission and completion times; the
   time-to-result is completion minus arrival and includes reading the
   result (eta, phi) back to the host;
@@ -108,14 +110,18 @@ def jonswap_device(n, kp, steepness, seed, depth=None, gamma=3.3, spread_s=10.0,
     phi = torch.fft.ifft2(P).real * (n * n)
     std = float(eta.std())
     scale = (2.0 * steepness / kp) / (4.0 * std) if std > 0 else 0.0
-    return (eta * scale).contiguous(), (phi * scale).contiguous(), 2 * math.pi / wp
+    eta, phi = (eta * scale).contiguous(), (phi * scale).contiguous()
+    # the library reads these on its own (non-blocking) streams: finish them here
+    torch.cuda.current_stream(eta.device).synchronize()
+    return eta, phi, 2 * math.pi / wp
 
 
 class DeviceBackend:
     """The server's device side: one ``HosField`` per admitted request, one
-    ``HosEnsemble`` over the active fields.  The request loop in ``Server``
-    only calls these methods, so that its queueing, admission, cancellation
-    and failure handling can be exercised without a GPU."""
+    persistent ``HosEnsemble`` over the active fields with a step budget per
+    member.  The request loop in ``Server`` only calls these methods, so that
+    its queueing, admission, cancellation and failure handling can be
+    exercised without a GPU."""
 
     def footprint(self, r):
         return HosField.footprint_bytes(r.n, r.n, r.order, r.precision)
@@ -136,13 +142,24 @@ class DeviceBackend:
             raise
         return f, tp / 50
 
-    def group(self, fields, dts):
-        return HosEnsemble(fields, dts)
+    def group(self, fields, dts, budgets):
+        """One persistent ensemble over the fields; member i takes at most
+        budgets[i] more steps, whatever number of steps is launched."""
+        g = HosEnsemble(fields, dts, mode="persistent")
+        try:
+            g.set_steps(budgets)
+        except Exception:
+            g.close()
+            raise
+        return g
 
-    def advance(self, group, steps):
-        """Advances every member; returns False when some member's state
-        became non-finite (the others are unaffected)."""
+    def launch(self, group, steps):
+        """Queues `steps` steps of every member that still has budget; returns at once."""
         group.step(steps)
+
+    def wait(self, group):
+        """Waits for the queued steps; returns False when some member's
+        state became non-finite (the others are unaffected)."""
         try:
             group.sync()
         except HosError as e:
@@ -150,6 +167,9 @@ class DeviceBackend:
                 raise
             return False
         return True
+
+    def remaining(self, group):
+        return group.remaining()
 
     def failed_step(self, f):
         return f.health()
@@ -170,15 +190,24 @@ class Server:
     if it is still queued).  With ``wait_for_more=True`` the loop idles for
     new submissions until ``stop()`` is called.
 
+    The loop runs the active fields in chunks: one launch of the persistent
+    ensemble per step, ``chunk`` steps at most and about ``chunk_seconds`` of
+    device time (sized from the previous chunk).  Every member has a step
+    budget on the device, so a request stops at exactly its own number of
+    steps inside a chunk and the others go on.  While a chunk runs, the loop
+    admits arrived requests (creates their fields and uploads their initial
+    seas); they join at the chunk's end, when the work list is re-planned.
+
     Each request ends with ``status``: "done" (result read back), "failed"
     (its state became non-finite; ``error`` says at which step; the other
     fields of the batch continue unaffected), "cancelled", or "rejected" (its
     footprint exceeds what the device offers with the server holding
     nothing)."""
 
-    def __init__(self, chunk=25, max_slots=4096, reserve_bytes=2 << 30, hbm_budget_bytes=None, keep_results=True,
-                 backend=None):
+    def __init__(self, chunk=64, chunk_seconds=0.05, max_slots=4096, reserve_bytes=2 << 30, hbm_budget_bytes=None,
+                 keep_results=True, backend=None):
         self.chunk = int(chunk)
+        self.chunk_seconds = float(chunk_seconds)
         self.max_slots = int(max_slots)
         self.reserve = int(reserve_bytes)
         self.budget = hbm_budget_bytes  # optional cap on what the server may hold
@@ -215,66 +244,52 @@ class Server:
     def run(self, requests=(), realtime=True, time_limit=None, wait_for_more=False):
         """Serve the requests (sorted by arrival) and any submitted meanwhile.
         With realtime, a request becomes visible at its arrival time on the
-        wall clock; otherwise all are visible at once.  Returns a metrics
-        dict."""
+        wall clock; otherwise all are visible at once.  With time_limit the
+        loop stops after that many seconds and reports what is still queued
+        or running as backlog.  Returns a metrics dict."""
         be = self.backend
         self._stop.clear()
         pending = sorted(requests, key=lambda r: r.arrival)
         submitted = len(pending)
-        active = []  # [req, field, dt, remaining]
+        active = []  # [req, field, dt, remaining steps]
+        staged = []  # admitted while a chunk ran; they join at its end
         done = []
         ended = []  # failed, cancelled and rejected requests
-        held = 0
+        st = {"held": 0}
         ens = None
         dirty = False
         gp_steps = 0.0
+        step_s = None  # seconds per step of the last chunk
         t0 = time.perf_counter()
 
         def retire(a, status, error=None):
-            nonlocal held
             r = a[0]
             r.status, r.error = status, error
             r.finished = time.perf_counter() - t0
             be.close(a[1])
-            held -= be.footprint(r)
+            st["held"] -= be.footprint(r)
             ended.append(r)
 
-        while True:
+        def intake():
+            nonlocal pending, submitted
             with self._mu:
                 if self._incoming:
                     submitted += len(self._incoming)
                     pending = sorted(pending + self._incoming, key=lambda r: r.arrival)
                     self._incoming = []
-                cancelled = set(self._cancelled)
-            if not (pending or active):
-                if wait_for_more and not self._stop.is_set():
-                    time.sleep(0.002)
-                    continue
-                break
+                return set(self._cancelled)
+
+        def admit(nslots):
+            """Admits visible requests in arrival order while they fit; a
+            request that does not fit does not block smaller ones behind it."""
             now = time.perf_counter() - t0
-            if time_limit is not None and now > time_limit:
-                break
-            # cancellation: queued requests leave at once, active ones here,
-            # at a chunk boundary
-            for r in [r for r in pending if r.rid in cancelled]:
-                r.status = "cancelled"
-                pending.remove(r)
-                ended.append(r)
-            gone = [a for a in active if a[0].rid in cancelled]
-            for a in gone:
-                retire(a, "cancelled")
-            if gone:
-                active = [a for a in active if a[0].rid not in cancelled]
-                dirty = True
-            # admission, in arrival order; a request that does not fit does
-            # not block smaller ones behind it
-            visible = [r for r in pending if (not realtime) or r.arrival <= now]
-            for r in visible:
-                if len(active) >= self.max_slots:
+            out = []
+            for r in [r for r in pending if (not realtime) or r.arrival <= now]:
+                if nslots + len(out) >= self.max_slots:
                     break
                 need = be.footprint(r)
-                if need > self._avail(held):
-                    if not active and held == 0:
+                if need > self._avail(st["held"]):
+                    if nslots + len(out) == 0 and st["held"] == 0:
                         r.status, r.error = "rejected", f"needs {need} bytes of device memory"
                         pending.remove(r)
                         ended.append(r)
@@ -282,23 +297,66 @@ class Server:
                 f, dt = be.open(r)
                 r.admitted = time.perf_counter() - t0
                 r.status = "active"
-                active.append([r, f, dt, r.steps])
-                held += need
+                out.append([r, f, dt, r.steps])
+                st["held"] += need
                 pending.remove(r)
+            return out
+
+        while True:
+            cancelled = intake()
+            if not (pending or active or staged):
+                if wait_for_more and not self._stop.is_set():
+                    time.sleep(0.002)
+                    continue
+                break
+            now = time.perf_counter() - t0
+            if time_limit is not None and now > time_limit:
+                break
+            # cancellation: queued requests leave at once, admitted ones here
+            for r in [r for r in pending if r.rid in cancelled]:
+                r.status = "cancelled"
+                pending.remove(r)
+                ended.append(r)
+            for group_list in (active, staged):
+                gone = [a for a in group_list if a[0].rid in cancelled]
+                for a in gone:
+                    retire(a, "cancelled")
+                    group_list.remove(a)
+                    dirty = True
+            if staged:
+                active += staged
+                staged = []
+                dirty = True
+            new = admit(len(active))
+            if new:
+                active += new
                 dirty = True
             if not active:
                 if pending and realtime:
                     time.sleep(max(0.0, min(0.002, pending[0].arrival - now)))
                 continue
-            if dirty:
+            if dirty or ens is None:
                 if ens is not None:
                     be.close(ens)
-                ens = be.group([a[1] for a in active], [a[2] for a in active])
+                ens = be.group([a[1] for a in active], [a[2] for a in active], [a[3] for a in active])
                 self.rebuilds += 1
                 dirty = False
-            steps = min(self.chunk, min(a[3] for a in active))
-            healthy = be.advance(ens, steps)
+            longest = max(a[3] for a in active)
+            steps = self.chunk if step_s is None else int(max(1, min(self.chunk, self.chunk_seconds / step_s)))
+            steps = min(steps, longest)
+            t_launch = time.perf_counter()
+            be.launch(ens, steps)
+            # while the chunk runs: admit what has arrived (joins at its end)
+            cancelled = intake()
+            staged += admit(len(active) + len(staged))
+            healthy = be.wait(ens)
+            step_s = (time.perf_counter() - t_launch) / steps
             self.chunks += 1
+            rem = be.remaining(ens)
+            for a, left in zip(active, rem):
+                took = a[3] - left
+                gp_steps += took * a[0].n * a[0].n
+                a[3] = left
             if not healthy:
                 bad = [(a, be.failed_step(a[1])) for a in active]
                 bad = [(a, s) for a, s in bad if s is not None]
@@ -306,10 +364,7 @@ class Server:
                     retire(a, "failed", f"state became non-finite at step {s}")
                 ids = {id(a) for a, _ in bad}
                 active = [a for a in active if id(a) not in ids]
-                dirty = True
-            for a in active:
-                a[3] -= steps
-                gp_steps += steps * a[0].n * a[0].n
+                dirty = dirty or bool(bad)
             finished = [a for a in active if a[3] == 0]
             for a in finished:
                 r, f = a[0], a[1]
@@ -319,7 +374,7 @@ class Server:
                 if self.keep_results:
                     r.result = res
                 be.close(f)
-                held -= be.footprint(r)
+                st["held"] -= be.footprint(r)
                 done.append(r)
             if finished:
                 active = [a for a in active if a[3] > 0]
@@ -329,17 +384,20 @@ class Server:
                 ens = None
         if ens is not None:
             be.close(ens)
-        for a in active:
+        backlog_running = len(active) + len(staged)
+        for a in active + staged:
             be.close(a[1])
         wall = time.perf_counter() - t0
         ttr = np.array([r.finished - r.arrival for r in done]) if done else np.zeros(0)
-        count = lambda st: sum(1 for r in ended if r.status == st)  # noqa: E731
+        count = lambda s: sum(1 for r in ended if r.status == s)  # noqa: E731
         return {
             "completed": len(done),
             "submitted": submitted,
             "failed": count("failed"),
             "cancelled": count("cancelled"),
             "rejected": count("rejected"),
+            "backlog_queued": len(pending),
+            "backlog_running": backlog_running,
             "wall_s": wall,
             "p50_s": float(np.percentile(ttr, 50)) if len(ttr) else None,
             "p99_s": float(np.percentile(ttr, 99)) if len(ttr) else None,

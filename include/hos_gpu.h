@@ -181,7 +181,34 @@ int hos_profile_stage(hos_handle h, double dt, int reps, hos_pass_stat* out, int
  * (it advances one field per process). Members must not be stepped on their
  * own while the ensemble exists; call hos_ensemble_sync before reading them. */
 typedef struct hos_ens* hos_ensemble;
+/* Classes mode (as above). */
 int hos_ensemble_create(const hos_handle* members, const double* dt, int n, hos_ensemble* out);
+/* mode HOS_ENS_CLASSES: as hos_ensemble_create.  mode HOS_ENS_PERSISTENT:
+ * one RK step of all members is ONE launch of a persistent kernel whose
+ * resident blocks take work items (blocks of one pass of one member) from a
+ * device list and wait, with a bounded wait, for the member's earlier
+ * passes; members of every grid, order, precision and depth share it.  Its
+ * members must have grids of 64..2048 points per direction and the default
+ * kernel shapes; each member ends bitwise as hos_step would leave it.  A
+ * wait that runs out makes hos_ensemble_sync return HOS_ERR_TIMEOUT (the
+ * members' states are then not valid until set again).  No counterpart in
+ * the reference (time_schemes_par.c:28-121 advances one field per process). */
+enum { HOS_ENS_CLASSES = 0, HOS_ENS_PERSISTENT = 1 };
+int hos_ensemble_create_ex(const hos_handle* members, const double* dt, int n, int mode, hos_ensemble* out);
+/* Persistent ensembles: per-member step budgets.  steps[i] >= 0 lets member
+ * i take that many more steps, after which its work items are skipped (its
+ * state and time stay as they are) until a new budget is set; -1 (the value
+ * after create) sets no limit.  get_remaining reads what is left (after the
+ * queued steps; it synchronises the ensemble's stream). */
+int hos_ensemble_set_steps(hos_ensemble e, const int* steps);
+int hos_ensemble_get_remaining(hos_ensemble e, int* steps);
+/* Bound of one wait of the persistent kernel, nanoseconds (default 2 s). */
+int hos_ensemble_set_wait_limit(hos_ensemble e, long long ns);
+/* Failure injection for tests: on != 0 re-plans the work list so that one
+ * task of the first member waits for one more completed item than its
+ * earlier passes have, so the wait runs out and the step fails with
+ * HOS_ERR_TIMEOUT; on = 0 restores the plan. */
+int hos_ensemble_withhold_dependency(hos_ensemble e, int on);
 int hos_ensemble_step(hos_ensemble e, int nsteps);
 int hos_ensemble_sync(hos_ensemble e);
 int hos_ensemble_info(hos_ensemble e, int* nclasses, int* launches_per_step);

@@ -16,9 +16,11 @@ class FakeField:
 
 
 class FakeGroup:
-    def __init__(self, fields):
+    def __init__(self, fields, budgets):
         self.fields = list(fields)
+        self.left = list(budgets)
         self.closed = False
+        self.ok = True
 
 
 class FakeBackend:
@@ -46,21 +48,30 @@ class FakeBackend:
         self.opened.append(f)
         return f, 0.1
 
-    def group(self, fields, dts):
+    def group(self, fields, dts, budgets):
         assert all(not f.closed for f in fields)
+        assert all(b > 0 for b in budgets)
         self.max_group = max(self.max_group, len(fields))
-        return FakeGroup(fields)
+        return FakeGroup(fields, budgets)
 
-    def advance(self, g, steps):
+    def launch(self, g, steps):
+        """Every member takes min(steps, its budget) steps, as the device does."""
         assert not g.closed
-        ok = True
-        for f in g.fields:
-            f.steps += steps
+        g.ok = True
+        for i, f in enumerate(g.fields):
+            took = min(steps, g.left[i])
+            f.steps += took
+            g.left[i] -= took
             if f.r.seed < 0 and f.steps >= -f.r.seed:
-                ok = False
+                g.ok = False
         if self.on_advance:
             self.on_advance(self)
-        return ok
+
+    def wait(self, g):
+        return g.ok
+
+    def remaining(self, g):
+        return list(g.left)
 
     def failed_step(self, f):
         return -f.r.seed if f.r.seed < 0 and f.steps >= -f.r.seed else None
