@@ -1211,7 +1211,12 @@ int build_ens_graph(hos_ens* E) {
 // The tasks of one RK step of every member (hos_persist.h): the passes
 // build_stage gives for each stage, re-shaped for PERSIST_THREADS threads,
 // then the step end.  Work items are dealt round by round over the members.
-constexpr int PERSIST_ITEM_CAP = 24;  // work items per task at most (more blocks per item above)
+// Blocks per work item: 1 for tasks of fewer than 16 blocks, nb/8 above, at
+// most 8.  An item is short (a member's step is a chain of ~50 tasks, each
+// waiting for the previous one's items), while a large pass still spreads
+// over many resident blocks and the number of items -- one atomic each --
+// stays a small fraction of the work.
+constexpr int PERSIST_MAX_PER_ITEM = 8;
 
 int size_index(int n, int base) {
   for (int s = 0; s < PERSIST_SIZES; s++)
@@ -1254,8 +1259,7 @@ int plan_persist(hos_ens* E) {
       ti.t.gx = gx;
       ti.t.gy = gy;
       const int nb = gx * gy;
-      const int items = std::min(nb, PERSIST_ITEM_CAP);
-      ti.t.per_item = (nb + items - 1) / items;
+      ti.t.per_item = std::max(1, std::min(PERSIST_MAX_PER_ITEM, nb / 8));
       ti.t.nitems = (nb + ti.t.per_item - 1) / ti.t.per_item;
       ti.t.dep = dep;
       ti.t.tw0 = tw0;

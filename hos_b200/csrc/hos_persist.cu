@@ -88,9 +88,10 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 2) k_persist(const __grid_con
   if (threadIdx.x == 0) s_epoch = *a.epoch;  // written by the previous launch's last block
   __syncthreads();
   const unsigned long long epoch = s_epoch;
+  int next_it = -1;  // thread 0: the item taken ahead, while the current one runs
   for (;;) {
     if (threadIdx.x == 0) {
-      int it = (int)atomicAdd(a.head, 1u);
+      int it = next_it >= 0 ? next_it : (int)atomicAdd(a.head, 1u);
       if (it >= a.nitems || ld_relaxed(a.err)) it = -1;
       int go = 0;
       if (it >= 0) {
@@ -120,6 +121,9 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 2) k_persist(const __grid_con
           }
         }
         __threadfence();
+        // take the next item now: the atomic's latency hides behind this
+        // item's work (items are still taken, and run, in list order)
+        if (go) next_it = (int)atomicAdd(a.head, 1u);
       }
       s_item = it;
       s_go = go;

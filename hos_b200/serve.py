@@ -190,6 +190,11 @@ class Server:
     if it is still queued).  With ``wait_for_more=True`` the loop idles for
     new submissions until ``stop()`` is called.
 
+    Admission takes requests in arrival order while their footprint fits the
+    free device memory and the work already admitted (remaining grid-point
+    steps over the measured rate) stays under ``max_inflight_s`` seconds;
+    a request that does not fit does not block smaller ones behind it.
+
     The loop runs the active fields in chunks: one launch of the persistent
     ensemble per step, ``chunk`` steps at most and about ``chunk_seconds`` of
     device time (sized from the previous chunk).  Every member has a step
@@ -205,9 +210,14 @@ class Server:
     nothing)."""
 
     def __init__(self, chunk=64, chunk_seconds=0.05, max_slots=4096, reserve_bytes=2 << 30, hbm_budget_bytes=None,
-                 keep_results=True, backend=None):
+                 keep_results=True, backend=None, max_inflight_s=4.0):
         self.chunk = int(chunk)
         self.chunk_seconds = float(chunk_seconds)
+        # admission also stops while the admitted work would take longer than
+        # this at the measured rate (grid-point-steps/s), so that under
+        # overload what is admitted finishes and the rest waits in the queue
+        self.max_inflight_s = float(max_inflight_s)
+        self.rate = 1e9
         self.max_slots = int(max_slots)
         self.reserve = int(reserve_bytes)
         self.budget = hbm_budget_bytes  # optional cap on what the server may hold
@@ -279,14 +289,20 @@ class Server:
                     self._incoming = []
                 return set(self._cancelled)
 
-        def admit(nslots):
+        def admit(inflight):
             """Admits visible requests in arrival order while they fit; a
-            request that does not fit does not block smaller ones behind it."""
+            request that does not fit does not block smaller ones behind it.
+            `inflight` lists the admitted [req, field, dt, remaining] entries."""
             now = time.perf_counter() - t0
             out = []
+            nslots = len(inflight)
+            work = sum(a[3] * a[0].n * a[0].n for a in inflight)
             for r in [r for r in pending if (not realtime) or r.arrival <= now]:
                 if nslots + len(out) >= self.max_slots:
                     break
+                rwork = r.steps * r.n * r.n
+                if nslots + len(out) > 0 and work + rwork > self.max_inflight_s * self.rate:
+                    continue
                 need = be.footprint(r)
                 if need > self._avail(st["held"]):
                     if nslots + len(out) == 0 and st["held"] == 0:
@@ -298,6 +314,7 @@ class Server:
                 r.admitted = time.perf_counter() - t0
                 r.status = "active"
                 out.append([r, f, dt, r.steps])
+                work += rwork
                 st["held"] += need
                 pending.remove(r)
             return out
@@ -327,7 +344,7 @@ class Server:
                 active += staged
                 staged = []
                 dirty = True
-            new = admit(len(active))
+            new = admit(active)
             if new:
                 active += new
                 dirty = True
@@ -348,15 +365,20 @@ class Server:
             be.launch(ens, steps)
             # while the chunk runs: admit what has arrived (joins at its end)
             cancelled = intake()
-            staged += admit(len(active) + len(staged))
+            staged += admit(active + staged)
             healthy = be.wait(ens)
-            step_s = (time.perf_counter() - t_launch) / steps
+            chunk_s = time.perf_counter() - t_launch
+            step_s = chunk_s / steps
             self.chunks += 1
             rem = be.remaining(ens)
+            chunk_gp = 0.0
             for a, left in zip(active, rem):
                 took = a[3] - left
-                gp_steps += took * a[0].n * a[0].n
+                chunk_gp += took * a[0].n * a[0].n
                 a[3] = left
+            gp_steps += chunk_gp
+            if chunk_gp > 0 and chunk_s > 0:
+                self.rate = 0.7 * self.rate + 0.3 * (chunk_gp / chunk_s)
             if not healthy:
                 bad = [(a, be.failed_step(a[1])) for a in active]
                 bad = [(a, s) for a, s in bad if s is not None]

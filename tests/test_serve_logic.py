@@ -188,3 +188,14 @@ def test_submit_from_another_thread_while_running():
     assert not th.is_alive()
     assert out["m"]["completed"] == 4 and out["m"]["submitted"] == 4
     assert all(r.result == (r.steps,) for r in late)
+
+
+def test_inflight_work_bound_keeps_the_rest_queued():
+    """With no room for admitted work beyond one request (max_inflight_s=0),
+    requests run one at a time, in arrival order, and every one completes."""
+    be = FakeBackend(1 << 30)
+    rs = reqs(4, steps=8)
+    m = Server(chunk=3, reserve_bytes=0, backend=be, max_inflight_s=0.0).run(rs, realtime=False)
+    assert m["completed"] == 4 and be.max_group == 1
+    assert [r.rid for r in sorted(rs, key=lambda r: r.admitted)] == [0, 1, 2, 3]
+    assert all(r.result == (r.steps,) for r in rs)
