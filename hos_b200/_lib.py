@@ -87,6 +87,7 @@ _SIGNATURES = {
     "hos_set_state_physical": (_I, [_H, _P, _P, _D]),
     "hos_get_state_physical": (_I, [_H, _P, _P]),
     "hos_step": (_I, [_H, _D, _I]),
+    "hos_step_adaptive": (_I, [_H, _D, ctypes.POINTER(_D), _D, _D, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "hos_sync": (_I, [_H]),
     "hos_health": (_I, [_H, ctypes.POINTER(ctypes.c_longlong)]),
     "hos_inject_alloc_failure": (None, [ctypes.c_long]),

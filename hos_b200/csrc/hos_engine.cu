@@ -84,6 +84,46 @@ __global__ void k_nonfinite(const double2* u, size_t n, int* flag) {
   if (bad && threadIdx.x == 0) atomicOr(flag, 1);
 }
 
+// ---------------------------------------------------------------- embedded error
+// Error estimate of an RK45 step: e = sum_s w_s k_s with w_s = dt (c_s - cs_s),
+// the difference between the 4th-order update the reference applies and the
+// 5th-order one of the same Dormand-Prince stages (time_schemes_par.c:183-235).
+// Each block writes max |e| and max |u| over its part of the packed state.
+constexpr int ERR_BLOCKS = 296;
+struct RkWeights {
+  double w[MAX_STAGES];
+};
+__global__ void __launch_bounds__(256) k_rk_err(const double2* __restrict__ k, int nst, size_t stride, RkWeights w,
+                                                const double2* __restrict__ u, size_t n, double* part) {
+  __shared__ double se[256], su[256];
+  double me = 0.0, mu = 0.0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    double ex = 0.0, ey = 0.0;
+    for (int s = 0; s < nst; s++) {
+      const double2 v = k[(size_t)s * stride + i];
+      ex += w.w[s] * v.x;
+      ey += w.w[s] * v.y;
+    }
+    me = fmax(me, sqrt(ex * ex + ey * ey));
+    const double2 q = u[i];
+    mu = fmax(mu, sqrt(q.x * q.x + q.y * q.y));
+  }
+  se[threadIdx.x] = me;
+  su[threadIdx.x] = mu;
+  __syncthreads();
+  for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+    if ((int)threadIdx.x < off) {
+      se[threadIdx.x] = fmax(se[threadIdx.x], se[threadIdx.x + off]);
+      su[threadIdx.x] = fmax(su[threadIdx.x], su[threadIdx.x + off]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = se[0];
+    part[2 * blockIdx.x + 1] = su[0];
+  }
+}
+
 // ---------------------------------------------------------------- step end
 // The step end (StepEndArgs, step_end_body) is in hos_kernels.cuh.
 __global__ void __launch_bounds__(256) k_step_end(const double* ham_part, int nparts, double* tdev, double dt,
@@ -351,6 +391,7 @@ struct hos_ctx {
   double2* ustg = nullptr;  // stage input of the current RK stage
   double2* zvbuf = nullptr; // Zvel outputs / operator scratch (allocated on first use)
   double* hpart = nullptr;  // Hamiltonian row partials (allocated on first use)
+  double* hpart_err = nullptr;  // adaptive-step error partials (allocated on first use)
   double2* zplain = nullptr;
   double* pplain = nullptr;
   void* tw[2][3] = {};  // [precision][nx, ny/2, ny] twiddle tables
@@ -984,7 +1025,7 @@ void release(hos_ctx* c) {
   if (c->graph) cudaGraphDestroy(c->graph);
   void* ptrs[] = {c->bad_step, c->u,    c->k,    c->zbuf,    c->phys,   c->ustage, c->ustg, c->zplain,   c->pplain,
                   c->tdev, c->trhs, c->rdev,    c->stepdev, c->actdev, c->flagdev, c->ham_part,
-                  c->ham_hist, c->t_hist, c->zvbuf, c->hpart, c->tw[0][0], c->tw[0][1], c->tw[0][2], c->tw[1][0], c->tw[1][1], c->tw[1][2]};
+                  c->ham_hist, c->t_hist, c->zvbuf, c->hpart, c->hpart_err, c->tw[0][0], c->tw[0][1], c->tw[0][2], c->tw[1][0], c->tw[1][1], c->tw[1][2]};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->st) cudaStreamDestroy(c->st);
@@ -1656,6 +1697,67 @@ int hos_step(hos_handle h, double dt, int nsteps) {
   int rc = build_graph(h, dt);
   if (rc) return rc;
   for (int i = 0; i < nsteps; i++) HOS_CK(cudaGraphLaunch(h->gexec, h->st));
+  return HOS_OK;
+}
+
+int hos_step_adaptive(hos_handle h, double t_end, double* dt, double rtol, double atol, int max_steps,
+                      int* accepted, int* rejected) {
+  if (!h || !dt) return fail(HOS_ERR_ARG, "null argument");
+  if (h->p.scheme != HOS_RK45DP) return fail(HOS_ERR_STATE, "adaptive steps need the RK45 scheme (scheme 1)");
+  if (!(*dt > 0.0) || !(rtol >= 0.0) || !(atol >= 0.0) || (rtol == 0.0 && atol == 0.0) || max_steps < 1)
+    return fail(HOS_ERR_ARG, "bad dt, tolerances or step limit");
+  // 5th-order weights of the pair (time_schemes_par.c:225-231); the update uses c (4th order), as the reference does
+  static const double cs[7] = {35.0 / 384.0, 0.0, 500.0 / 1113.0, 125.0 / 192.0, -2187.0 / 6784.0, 11.0 / 84.0, 0.0};
+  if (!h->hpart_err) {
+    int rc = dalloc(&h->hpart_err, (size_t)2 * ERR_BLOCKS * sizeof(double));
+    if (rc) return rc;
+  }
+  int acc = 0, rej = 0;
+  double t = 0.0;
+  long long step0 = 0;
+  HOS_CK(cudaMemcpyAsync(&t, h->tdev, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  HOS_CK(cudaStreamSynchronize(h->st));
+  std::vector<double> part(2 * ERR_BLOCKS);
+  const double span = std::max(std::fabs(t_end), std::fabs(t));
+  double dtry = *dt;
+  while (t_end - t > 1e-12 * span && acc + rej < max_steps) {
+    const double dts = std::min(dtry, t_end - t);
+    HOS_CK(cudaMemcpyAsync(&step0, h->stepdev, sizeof(long long), cudaMemcpyDeviceToHost, h->st));
+    HOS_CK(cudaMemcpyAsync(h->ustage, h->u, 2 * h->fsz * sizeof(double2), cudaMemcpyDeviceToDevice, h->st));
+    int rc = enqueue_step(h, dts);
+    if (rc) return rc;
+    RkWeights w{};
+    for (int s = 0; s < h->nst; s++) w.w[s] = dts * (h->c[s] - cs[s]);
+    k_rk_err<<<ERR_BLOCKS, 256, 0, h->st>>>(h->k, h->nst, 2 * h->fsz, w, h->u, 2 * h->fsz, h->hpart_err);
+    HOS_CK(cudaGetLastError());
+    HOS_CK(cudaMemcpyAsync(part.data(), h->hpart_err, part.size() * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    HOS_CK(cudaStreamSynchronize(h->st));
+    double me = 0.0, mu = 0.0;
+    for (int b = 0; b < ERR_BLOCKS; b++) {
+      me = std::max(me, part[2 * b]);
+      mu = std::max(mu, part[2 * b + 1]);
+    }
+    const double err = me / (atol + rtol * mu);
+    if (!std::isfinite(err)) return fail(HOS_ERR_NONFINITE, "adaptive step at t=%g: error estimate not finite", t);
+    if (err <= 1.0) {
+      acc++;
+      t += dts;
+    } else {  // rejected: the state, time and step count go back to the step's start
+      rej++;
+      HOS_CK(cudaMemcpyAsync(h->u, h->ustage, 2 * h->fsz * sizeof(double2), cudaMemcpyDeviceToDevice, h->st));
+      HOS_CK(cudaMemcpyAsync(h->tdev, &t, sizeof(double), cudaMemcpyHostToDevice, h->st));
+      HOS_CK(cudaMemcpyAsync(h->stepdev, &step0, sizeof(long long), cudaMemcpyHostToDevice, h->st));
+      HOS_CK(cudaStreamSynchronize(h->st));
+    }
+    // elementary controller for a 4th/5th-order pair: safety 0.9, growth in [0.2, 5]
+    const double fac = err == 0.0 ? 5.0 : std::min(5.0, std::max(0.2, 0.9 * std::pow(err, -0.2)));
+    dtry = dts * fac;
+  }
+  // the time the host tracked is the device's to the last rounding: keep the device's
+  *dt = dtry;
+  if (accepted) *accepted = acc;
+  if (rejected) *rejected = rej;
+  if (t_end - t > 1e-12 * span) return fail(HOS_ERR_STATE, "adaptive steps stopped at t=%g after %d attempts", t, acc + rej);
   return HOS_OK;
 }
 

@@ -10,6 +10,7 @@ HosField method        reference routine
 ``set_state_physical`` fft_2d x2 + Dealias x2 (main_2d_par.c:258-262)
 ``state_physical``     ifft_2d x2 (main_2d_par.c:310-311)
 ``step``               sol_update_RK (time_schemes_par.c:28-121), n times
+``step_adaptive``      RK45 pair of Setup_TimeScheme(1) with step control
 ``rhs``                rhs_hos (hosm_2d_par.c:138-235)
 ``fft_2d``/``ifft_2d`` fft_routines_2d_par.c:21-103
 ``energy_history``     Hamiltonian at stage 0 (hosm_2d_par.c:462-523),
@@ -168,6 +169,15 @@ class HosField:
     # ------------------------------------------------------------ time stepping
     def step(self, dt, nsteps=1):
         _lib.check(self._lib.hos_step(self._h, float(dt), int(nsteps)))
+
+    def step_adaptive(self, t_end, dt, rtol=1e-8, atol=1e-12, max_steps=100000):
+        """Adaptive RK45 steps (scheme "rk45") from the field's time to t_end;
+        returns (next proposed dt, kept steps, rejected steps)."""
+        d = ctypes.c_double(float(dt))
+        acc, rej = ctypes.c_int(), ctypes.c_int()
+        _lib.check(self._lib.hos_step_adaptive(self._h, float(t_end), ctypes.byref(d), float(rtol), float(atol),
+                                               int(max_steps), ctypes.byref(acc), ctypes.byref(rej)))
+        return d.value, acc.value, rej.value
 
     def sync(self):
         """Waits for queued steps; raises HosError (code HOS_ERR_NONFINITE)

@@ -105,6 +105,21 @@ int hos_get_state_physical(hos_handle h, double* eta, double* phi);
  * time_schemes_par.c:28-121, called nsteps times).  Asynchronous with
  * respect to the host; hos_sync waits. */
 int hos_step(hos_handle h, double dt, int nsteps);
+/* Adaptive steps with the reference's Dormand-Prince pair (scheme 1,
+ * Setup_TimeScheme, time_schemes_par.c:183-235), from the handle's time to
+ * t_end.  Each step advances with the 4th-order weights c, as the
+ * reference's fixed-step scheme 1 does; the 5th-order weights cs, which the
+ * reference computes but never uses, give the error estimate
+ * e = dt sum_s (c_s - cs_s) k_s.  A step is kept when
+ * max|e| <= atol + rtol max|u| (complex moduli over the packed state u after
+ * the step); otherwise the state, time and step count return to the step's
+ * start.  The next step is dt * min(5, max(0.2, 0.9 (max|e| / tol)^(-1/5))),
+ * and the last is shortened to land on t_end.  *dt is the first trial step
+ * on entry and the next proposed step on return.  Synchronous; the energy
+ * record holds the kept steps.  HOS_ERR_STATE if the scheme is not 1 or
+ * max_steps attempts did not reach t_end. */
+int hos_step_adaptive(hos_handle h, double t_end, double* dt, double rtol, double atol, int max_steps,
+                      int* accepted, int* rejected);
 /* Waits for the handle's work.  Returns HOS_ERR_NONFINITE when a step's
  * energy was NaN or Inf, i.e. the state became non-finite (set on the device
  * by the step-end reduction; cleared by the next hos_set_state_*). */

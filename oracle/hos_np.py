@@ -50,6 +50,11 @@ _SCHEMES = {
 }
 
 
+# 5th-order weights of the RK45 pair (time_schemes_par.c:225-231); the
+# reference computes them and never uses them.
+RK45_CS = [35.0 / 384.0, 0.0, 500.0 / 1113.0, 125.0 / 192.0, -2187.0 / 6784.0, 11.0 / 84.0, 0.0]
+
+
 def butcher(scheme: int):
     """Return (b, c) for a reference scheme id; b[s][p] for p < s."""
     if scheme not in _SCHEMES:
@@ -241,4 +246,36 @@ class HosNumpy:
         for s in range(len(c)):
             ne = ne + dt * c[s] * ks[s][0]
             npf = npf + dt * c[s] * ks[s][1]
+        self.last_stages = ks
         return ne, npf, t + dt, H
+
+    def advance_adaptive(self, heta, hphi, t, t_end, dt, rtol, atol, max_steps=100000):
+        """Adaptive steps with the RK45 pair, the step control of the
+        library's hos_step_adaptive restated: update with the 4th-order
+        weights c (as scheme 1 of the reference), error e = dt sum (c - cs) k,
+        keep the step when max|e| <= atol + rtol max|u_new|, next step
+        dt * min(5, max(0.2, 0.9 (max|e|/tol)^(-1/5))), the last one shortened
+        to land on t_end.  Returns (heta, hphi, t, next dt, kept energies,
+        kept, rejected)."""
+        _, c = butcher(1)
+        span = max(abs(t_end), abs(t))
+        acc = rej = 0
+        H = []
+        while t_end - t > 1e-12 * span and acc + rej < max_steps:
+            dts = min(dt, t_end - t)
+            ne, npf, _, h = self.step(heta, hphi, t, dts, 1)
+            ks = self.last_stages
+            ee = sum(dts * (c[s] - RK45_CS[s]) * ks[s][0] for s in range(7))
+            ep = sum(dts * (c[s] - RK45_CS[s]) * ks[s][1] for s in range(7))
+            me = max(np.max(np.abs(ee)), np.max(np.abs(ep)))
+            mu = max(np.max(np.abs(ne)), np.max(np.abs(npf)))
+            err = me / (atol + rtol * mu)
+            if err <= 1.0:
+                acc += 1
+                heta, hphi, t = ne, npf, t + dts
+                H.append(h)
+            else:
+                rej += 1
+            fac = 5.0 if err == 0.0 else min(5.0, max(0.2, 0.9 * err ** -0.2))
+            dt = dts * fac
+        return heta, hphi, t, dt, np.array(H), acc, rej

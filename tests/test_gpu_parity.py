@@ -304,3 +304,27 @@ def test_one_step_2048_vs_reference():
         f.step(dt, 1)
         u, _ = f.state_spectral()
     assert rel(u[0], ref_u[0]) < TOL_STEPS and rel(u[1], ref_u[1]) < TOL_STEPS
+
+
+def test_adaptive_rk45_matches_restatement():
+    """hos_step_adaptive against the restated step control (oracle/hos_np.py:
+    advance_adaptive): the same kept and rejected steps, the same next dt,
+    and the state and the kept steps' energies to 1e-10."""
+    n, M = 64, 4
+    eta, phi, info = ic.jonswap(n, n, kp=8.0, steepness=0.1, seed=31)
+    tp = info["Tp"]
+    hn = HosNumpy(n, n, 2 * math.pi, 2 * math.pi, 1.0, M)
+    e, p = hn.init_state(eta, phi)
+    # a first step far too large: the controller must reject and shrink it
+    re, rp, rt, rdt, rH, racc, rrej = hn.advance_adaptive(e, p, 0.0, tp, 2.0 * tp, 1e-7, 1e-14)
+    assert rrej >= 1
+    with HosField(n, n, order=M, scheme="rk45") as f:
+        f.set_state_physical(eta, phi)
+        dt, acc, rej = f.step_adaptive(tp, 2.0 * tp, rtol=1e-7, atol=1e-14)
+        u, t = f.state_spectral()
+        _, H = f.energy_history()
+    assert (acc, rej) == (racc, rrej)
+    assert abs(dt - rdt) <= 1e-9 * rdt
+    assert abs(t - rt) <= 1e-12 * tp
+    assert rel(u[0], re) < TOL_STEPS and rel(u[1], rp) < TOL_STEPS
+    assert len(H) == acc and np.max(np.abs(H - rH)) / np.max(np.abs(rH)) < TOL_STEPS
