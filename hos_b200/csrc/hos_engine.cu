@@ -619,6 +619,16 @@ struct PassRec {
   YFwdArgs yf{};
 };
 
+// Column-strip staging of the y-inverse passes: cp.async (default) or plain
+// loads and shared stores (HOS_STRIP=plain in the environment).
+bool strip_plain() {
+  static const bool on = [] {
+    const char* s = getenv("HOS_STRIP");
+    return s && s[0] == 'p';
+  }();
+  return on;
+}
+
 // Builds one RK stage (or one bare RHS evaluation when rhs_only).
 // zvel_out: when set, the stage ends after the W recursion and Zvel's four
 // spectral outputs W^(M), W^(M-2), (W^2)^(M), (W^2)^(M-2) (hosm_2d_par.c:240-445)
@@ -678,6 +688,7 @@ void build_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, doub
   ya.rows_in = c->h + 1;
   ya.rows_dev = rows_dev;
   ya.phys = c->phys;
+  ya.plain_strip = strip_plain();
   int nj = 0;
   ya.jobs[nj++] = YJob{0, 0, c->ETA()};
   ya.jobs[nj++] = YJob{0, 1, c->ETAY()};
@@ -745,6 +756,7 @@ void build_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, doub
     yl.z = c->zbuf;
     yl.rows_in = c->h + 1;
     yl.phys = c->phys;
+    yl.plain_strip = strip_plain();
     int nl = 0;
     for (int j = 1; j <= M - n; j++) yl.jobs[nl++] = YJob{1 + j - 1, 0, c->D(n + 1, j)};
     yl.ycount = nl;
@@ -1101,6 +1113,7 @@ struct hos_ens {
   size_t psmem = 0;
   int ntasks = 0;
   int withhold = 0;      // test hook: one task waits for an item that never exists
+  int minb = 2;          // resident blocks per SM the persistent kernel is compiled for
 };
 
 namespace {
@@ -1252,11 +1265,12 @@ int build_ens_graph(hos_ens* E) {
 // The tasks of one RK step of every member (hos_persist.h): the passes
 // build_stage gives for each stage, re-shaped for PERSIST_THREADS threads,
 // then the step end.  Work items are dealt round by round over the members.
-// Blocks per work item: 1 for tasks of fewer than 16 blocks, nb/8 above, at
-// most 8.  An item is short (a member's step is a chain of ~50 tasks, each
-// waiting for the previous one's items), while a large pass still spreads
-// over many resident blocks and the number of items -- one atomic each --
-// stays a small fraction of the work.
+// Blocks per work item.  The members' current tasks together should offer
+// about twice as many items as there are resident blocks: a task gets
+// ceil(2 * resident / members) items (at least 1), so one field alone spreads
+// each pass over the whole GPU and many fields take few, larger items each
+// (fewer atomics).  An item holds at most 8 blocks, so that the chain of a
+// member's ~50 dependent tasks stays short.
 constexpr int PERSIST_MAX_PER_ITEM = 8;
 
 int size_index(int n, int base) {
@@ -1278,6 +1292,9 @@ int plan_persist(hos_ens* E) {
     return off;
   };
   const int nm = (int)E->mem.size();
+  int sms = 0;
+  HOS_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, E->mem[0]->device));
+  const int target_items = std::max(1, (2 * 2 * sms + nm - 1) / nm);  // about 2 resident blocks per SM
   std::vector<std::vector<TaskImg>> per(nm);
   std::vector<long long> member_items(nm, 0);
   size_t smem = 0;
@@ -1300,7 +1317,7 @@ int plan_persist(hos_ens* E) {
       ti.t.gx = gx;
       ti.t.gy = gy;
       const int nb = gx * gy;
-      ti.t.per_item = std::max(1, std::min(PERSIST_MAX_PER_ITEM, nb / 8));
+      ti.t.per_item = std::max(1, std::min(PERSIST_MAX_PER_ITEM, (nb + target_items - 1) / target_items));
       ti.t.nitems = (nb + ti.t.per_item - 1) / ti.t.per_item;
       ti.t.dep = dep;
       ti.t.tw0 = tw0;
@@ -1355,7 +1372,7 @@ int plan_persist(hos_ens* E) {
   // the global list: task k of every member, then task k + 1, ...
   std::vector<PTask> tasks;
   std::vector<size_t> arg_off;
-  std::vector<int> item_task;
+  std::vector<int4> item_task;
   size_t kmax = 0;
   for (auto& v : per) kmax = std::max(kmax, v.size());
   for (size_t k = 0; k < kmax; k++)
@@ -1363,18 +1380,21 @@ int plan_persist(hos_ens* E) {
       if (k >= per[f].size()) continue;
       PTask t = per[f][k].t;
       t.first_item = (int)item_task.size();
-      for (int i = 0; i < t.nitems; i++) item_task.push_back((int)tasks.size());
+      for (int i = 0; i < t.nitems; i++)
+        item_task.push_back(make_int4((int)tasks.size(), f, (int)t.dep, (int)member_items[f]));
       tasks.push_back(t);
       arg_off.push_back(per[f][k].arg_off);
     }
   if (item_task.size() > (size_t)0x7fffffff) return fail(HOS_ERR_ARG, "persistent ensemble: too many work items");
+  for (long long mi : member_items)
+    if (mi > 0x7fffffffLL) return fail(HOS_ERR_ARG, "persistent ensemble: too many work items in one member's step");
 
   // one device buffer: counters | done[nm] | member_items[nm] | remaining[nm] | tasks | item_task | argument blob
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
   const size_t o_cnt = 0, o_done = 256, o_mi = al(o_done + nm * 8), o_rem = al(o_mi + nm * 8);
   const size_t o_tasks = al(o_rem + nm * 4);
   const size_t o_items = al(o_tasks + tasks.size() * sizeof(PTask));
-  const size_t o_blob = al(o_items + item_task.size() * sizeof(int));
+  const size_t o_blob = al(o_items + item_task.size() * sizeof(int4));
   const size_t total = o_blob + blob.size();
   if (E->pbuf) cudaFree(E->pbuf);
   E->pbuf = nullptr;
@@ -1386,13 +1406,13 @@ int plan_persist(hos_ens* E) {
   std::memcpy(img.data() + o_mi, member_items.data(), nm * 8);
   std::memset(img.data() + o_rem, 0xff, nm * 4);  // -1: no step budget
   std::memcpy(img.data() + o_tasks, tasks.data(), tasks.size() * sizeof(PTask));
-  std::memcpy(img.data() + o_items, item_task.data(), item_task.size() * sizeof(int));
+  std::memcpy(img.data() + o_items, item_task.data(), item_task.size() * sizeof(int4));
   HOS_CK(cudaMemcpy(base, img.data(), img.size(), cudaMemcpyHostToDevice));
   HOS_CK(cudaMemcpy(base + o_blob, blob.data(), blob.size(), cudaMemcpyHostToDevice));
 
   PersistArgs& a = E->pa;
   a.tasks = reinterpret_cast<const PTask*>(base + o_tasks);
-  a.item_task = reinterpret_cast<const int*>(base + o_items);
+  a.item_info = reinterpret_cast<const int4*>(base + o_items);
   a.nitems = (int)item_task.size();
   a.done = reinterpret_cast<unsigned long long*>(base + o_done);
   a.member_items = reinterpret_cast<const long long*>(base + o_mi);
@@ -1406,13 +1426,19 @@ int plan_persist(hos_ens* E) {
   if (a.wait_limit_ns <= 0) a.wait_limit_ns = 2000000000LL;  // 2 s
   E->ntasks = (int)tasks.size();
 
+  // 3 resident blocks per SM (80 registers a thread) when every grid is at
+  // most 256 points per direction, where more warps pay more than the
+  // spills of the heavier bodies cost; 2 otherwise.  HOS_PERSIST_MINB=2|3 in
+  // the environment overrides.
+  int maxn = 0;
+  for (hos_ctx* c : E->mem) maxn = std::max(maxn, std::max(c->nx, c->ny));
+  E->minb = maxn <= 256 ? 3 : 2;
+  if (const char* ev = getenv("HOS_PERSIST_MINB")) E->minb = (ev[0] == '3') ? 3 : 2;
   // resident blocks: the launch is cooperative, so all of them must fit at once
   smem = std::max(smem, (size_t)16);
-  HOS_CK(persist_set_smem(smem));
+  HOS_CK(persist_set_smem(smem, E->minb));
   int per_sm = 0;
-  HOS_CK(persist_occupancy(&per_sm, smem));
-  int sms = 0;
-  HOS_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, E->mem[0]->device));
+  HOS_CK(persist_occupancy(&per_sm, smem, E->minb));
   if (per_sm < 1) return fail(HOS_ERR_ARG, "persistent ensemble: kernel does not fit an SM");
   E->pblocks = per_sm * sms;
   E->psmem = smem;
@@ -2081,7 +2107,7 @@ int hos_ensemble_create_ex(const hos_handle* members, const double* dt, int n, i
 int hos_ensemble_step(hos_ensemble e, int nsteps) {
   if (!e || nsteps < 0) return fail(HOS_ERR_ARG, "bad argument");
   if (e->mode == HOS_ENS_PERSISTENT) {
-    for (int i = 0; i < nsteps; i++) HOS_CK(persist_launch(e->pa, e->pblocks, e->psmem, e->st));
+    for (int i = 0; i < nsteps; i++) HOS_CK(persist_launch(e->pa, e->pblocks, e->psmem, e->st, e->minb));
     return HOS_OK;
   }
   for (int i = 0; i < nsteps; i++) HOS_CK(cudaGraphLaunch(e->gexec, e->st));

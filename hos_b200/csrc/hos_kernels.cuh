@@ -510,6 +510,7 @@ struct YInvArgs {
   int nx_in[MAX_TERMS];
   void* vout;
   int store_job0;  // 0 when the fused job-0 result has no other reader
+  int plain_strip; // stage the column strip with loads and shared stores instead of cp.async
 };
 
 template <typename T, int H, int E, int MODE>
@@ -539,12 +540,30 @@ __device__ __forceinline__ void yinv_body(const YInvArgs& a, int bx, int by, int
     const int nin = G * (a.rows_dev ? *a.rows_dev : a.rows_in);
     const int ntot = G * (H + 1);
     const int lg = __ffs(G) - 1;  // G is a power of two
-    for (int q = threadIdx.x; q < ntot; q += nthreads) {
-      const int ky = q >> lg, g = q & (G - 1);
-      const bool live = q < nin;
-      cp_async_elem(&sm[(size_t)g * a.lp + ky], live ? zs + (size_t)ky * nx + ix0 + g : zs, live);
+    if (a.plain_strip) {
+      // every load in flight first, then the shared stores: an asynchronous
+      // copy costs one shared-memory wavefront per 32-byte global sector,
+      // these conflict-free stores one per 128 bytes.  A thread holds at
+      // most ceil((H+1)/P) = E+1 elements.
+      C buf[E + 1];
+#pragma unroll
+      for (int j = 0; j <= E; j++) {
+        const int q = threadIdx.x + j * nthreads;
+        buf[j] = q < nin ? __ldg(zs + (size_t)(q >> lg) * nx + ix0 + (q & (G - 1))) : mkc((T)0, (T)0);
+      }
+#pragma unroll
+      for (int j = 0; j <= E; j++) {
+        const int q = threadIdx.x + j * nthreads;
+        if (q < ntot) sm[(size_t)(q & (G - 1)) * a.lp + (q >> lg)] = buf[j];
+      }
+    } else {
+      for (int q = threadIdx.x; q < ntot; q += nthreads) {
+        const int ky = q >> lg, g = q & (G - 1);
+        const bool live = q < nin;
+        cp_async_elem(&sm[(size_t)g * a.lp + ky], live ? zs + (size_t)ky * nx + ix0 + g : zs, live);
+      }
+      cp_async_wait_all();
     }
-    cp_async_wait_all();
   }
   __syncthreads();
   // complex-to-real preprocessing: c[k] = Xe + i Xo (packing of a length-Ny

@@ -3,6 +3,7 @@
 // the member's earlier passes, runs the pass body on the item's blocks and
 // counts the item done.
 #include <cstdint>
+#include <cstdlib>
 
 #include "hos_kernels.cuh"
 #include "hos_persist.h"
@@ -80,10 +81,11 @@ __device__ __forceinline__ long long now_ns() {
   return t;
 }
 
-__global__ void __launch_bounds__(PERSIST_THREADS, 2) k_persist(const __grid_constant__ PersistArgs a) {
+template <int MINB>
+__global__ void __launch_bounds__(PERSIST_THREADS, MINB) k_persist(const __grid_constant__ PersistArgs a) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  __shared__ int s_item;
-  __shared__ int s_go;
+  __shared__ PTask s_task;  // the current item's task, read once by thread 0
+  __shared__ int s_item, s_go, s_left;
   __shared__ unsigned long long s_epoch;
   if (threadIdx.x == 0) s_epoch = *a.epoch;  // written by the previous launch's last block
   __syncthreads();
@@ -95,14 +97,16 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 2) k_persist(const __grid_con
       if (it >= a.nitems || ld_relaxed(a.err)) it = -1;
       int go = 0;
       if (it >= 0) {
-        const PTask& k = a.tasks[a.item_task[it]];
-        const unsigned long long target =
-            epoch * (unsigned long long)a.member_items[k.member] + (unsigned long long)k.dep;
-        unsigned long long seen = ld_acquire(&a.done[k.member]);
+        // one load gives the task, the member and the wait target
+        const int4 inf = __ldg(&a.item_info[it]);
+        s_task = a.tasks[inf.x];
+        s_left = a.remaining[inf.y];
+        const unsigned long long target = epoch * (unsigned long long)(unsigned)inf.w + (unsigned long long)(unsigned)inf.z;
+        unsigned long long seen = ld_acquire(&a.done[inf.y]);
         go = 1;
         if (seen < target) {
           const long long t0 = now_ns();
-          while ((seen = ld_acquire(&a.done[k.member])) < target) {
+          while ((seen = ld_acquire(&a.done[inf.y])) < target) {
             if (ld_relaxed(a.err)) {
               go = 0;
               break;
@@ -110,17 +114,16 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 2) k_persist(const __grid_con
             if (now_ns() - t0 > a.wait_limit_ns) {
               if (atomicCAS(a.err, 0, 1) == 0) {
                 a.err_info[0] = it;
-                a.err_info[1] = k.member;
+                a.err_info[1] = inf.y;
                 a.err_info[2] = (long long)target;
                 a.err_info[3] = (long long)seen;
               }
               go = 0;
               break;
             }
-            __nanosleep(200);
+            __nanosleep(100);
           }
         }
-        __threadfence();
         // take the next item now: the atomic's latency hides behind this
         // item's work (items are still taken, and run, in list order)
         if (go) next_it = (int)atomicAdd(a.head, 1u);
@@ -128,10 +131,11 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 2) k_persist(const __grid_con
       s_item = it;
       s_go = go;
     }
+    // the barrier orders every thread's reads after thread 0's acquire
     __syncthreads();
     const int it = s_item;
     if (it < 0 || !s_go) break;
-    const PTask& k = a.tasks[a.item_task[it]];
+    const PTask& k = s_task;
     const int local = it - k.first_item;
     const int b0 = local * k.per_item;
     const int nb = k.gx * k.gy;
@@ -139,7 +143,7 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 2) k_persist(const __grid_con
     // a member whose step budget is spent skips its items (they still count
     // as done); the budget only changes in the member's step end, the last
     // task of its step, so every item of one launch sees the same value
-    const int left = a.remaining[k.member];
+    const int left = s_left;
     if (left == 0) {
       // nothing to do
     } else if (k.body == PC_STEP_END * PERSIST_SIZES) {
@@ -155,10 +159,14 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 2) k_persist(const __grid_con
         __syncthreads();  // the next block of the item reuses the shared memory
       }
     }
-    // the item's writes are visible device-wide before it is counted done
-    __threadfence();
+    // the item's writes are visible device-wide before it is counted done:
+    // the barrier orders every thread's writes before thread 0's fence,
+    // which is cumulative, and the count comes after the fence
     __syncthreads();
-    if (threadIdx.x == 0) atomicAdd(&a.done[k.member], 1ull);
+    if (threadIdx.x == 0) {
+      __threadfence();
+      atomicAdd(&a.done[k.member], 1ull);
+    }
   }
   // the last block out resets the counters for the next launch
   __syncthreads();
@@ -182,7 +190,9 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 2) k_persist(const __grid_con
 
 }  // namespace
 
-cudaError_t persist_launch(const PersistArgs& a, int blocks, size_t smem, cudaStream_t st) {
+const void* persist_fn(int minb) { return minb == 3 ? (const void*)k_persist<3> : (const void*)k_persist<2>; }
+
+cudaError_t persist_launch(const PersistArgs& a, int blocks, size_t smem, cudaStream_t st, int minb) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(blocks);
   cfg.blockDim = dim3(PERSIST_THREADS);
@@ -193,15 +203,16 @@ cudaError_t persist_launch(const PersistArgs& a, int blocks, size_t smem, cudaSt
   at[0].val.cooperative = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_persist, a);
+  if (minb == 3) return cudaLaunchKernelEx(&cfg, k_persist<3>, a);
+  return cudaLaunchKernelEx(&cfg, k_persist<2>, a);
 }
 
-cudaError_t persist_occupancy(int* blocks_per_sm, size_t smem) {
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_persist, PERSIST_THREADS, smem);
+cudaError_t persist_occupancy(int* blocks_per_sm, size_t smem, int minb) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, persist_fn(minb), PERSIST_THREADS, smem);
 }
 
-cudaError_t persist_set_smem(size_t smem) {
-  return cudaFuncSetAttribute(k_persist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+cudaError_t persist_set_smem(size_t smem, int minb) {
+  return cudaFuncSetAttribute(persist_fn(minb), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
 }  // namespace hos

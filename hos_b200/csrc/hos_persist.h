@@ -60,7 +60,7 @@ struct PTask {
 
 struct PersistArgs {
   const PTask* tasks;
-  const int* item_task;              // task of every item, in list order
+  const int4* item_info;             // per item, in list order: task, member, dep of the task, items of the member's step
   int nitems;
   unsigned long long* done;          // per member: items completed, over all launches
   const long long* member_items;     // per member: items of one step
@@ -74,12 +74,15 @@ struct PersistArgs {
   long long wait_limit_ns;           // bound of one wait
 };
 
+// The kernel is compiled for 2 resident blocks per SM (up to 128 registers a
+// thread) and for 3 (up to 80: more warps, the heavier pass bodies spill);
+// `minb` selects one.
 // Launches one step of the persistent kernel (cooperative launch of
 // `blocks` blocks with `smem` bytes of dynamic shared memory).
-cudaError_t persist_launch(const PersistArgs& a, int blocks, size_t smem, cudaStream_t st);
+cudaError_t persist_launch(const PersistArgs& a, int blocks, size_t smem, cudaStream_t st, int minb);
 // Resident blocks per SM of the persistent kernel for `smem` bytes.
-cudaError_t persist_occupancy(int* blocks_per_sm, size_t smem);
+cudaError_t persist_occupancy(int* blocks_per_sm, size_t smem, int minb);
 // Raises the kernel's dynamic shared memory limit to `smem` bytes.
-cudaError_t persist_set_smem(size_t smem);
+cudaError_t persist_set_smem(size_t smem, int minb);
 
 }  // namespace hos
