@@ -61,7 +61,7 @@ def parse():
     ap.add_argument("--no-configs", action="store_true")
     ap.add_argument("--ensemble-fields", type=int, default=256)
     ap.add_argument("--ensemble-steps", type=int, default=500)
-    ap.add_argument("--ensemble-mode", default="persistent", choices=["persistent", "classes"])
+    ap.add_argument("--ensemble-mode", default="classes", choices=["persistent", "classes"])
     ap.add_argument("--serve-utilization", type=float, default=0.7)
     ap.add_argument("--serve-duration", type=float, default=20.0)
     ap.add_argument("--serve-limit", type=float, default=80.0)
@@ -700,8 +700,13 @@ def run_ours(args, rep):
     }
     if "ensemble" in line:
         e = line["ensemble"]
-        summ["ensemble"] = {k: e.get(k) for k in ("fields", "launches_per_step", "grid_point_steps_per_s",
+        summ["ensemble"] = {k: e.get(k) for k in ("fields", "mode", "launches_per_step", "grid_point_steps_per_s",
                                                   "speedup_vs_sequential_fp64")}
+        o = e.get("other_mode", {})
+        seq_gps = e.get("sequential_fp64_grid_point_steps_per_s")
+        summ["ensemble_" + str(o.get("mode"))] = {
+            "launches_per_step": o.get("launches_per_step"), "grid_point_steps_per_s": o.get("grid_point_steps_per_s"),
+            "speedup_vs_sequential_fp64": (o["grid_point_steps_per_s"] / seq_gps) if seq_gps and o else None}
     if "serving" in line:
         sv = line["serving"]
         summ["serving"] = {k: sv.get(k) for k in ("arrival_rate_per_s", "completed", "p50_s", "p99_s",

@@ -119,6 +119,7 @@ enum { YF_PLAIN = 0, YF_LEVEL = 1, YF_RHS = 2 };
 // ---------------------------------------------------------------- x inverse
 struct XInvArgs {
   Geo geo;
+  const int* remaining; // batched launches: the member's step budget (0: skip the pass); nullptr: no budget
   int ycount;           // batched launches: blocks with blockIdx.y >= ycount have no work
   int rows;             // ky rows that may be nonzero in the input
   const int* rows_dev;  // if set, overrides rows (active rows of the state, kept on the device)
@@ -216,6 +217,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_xinv(const __grid_constant__
   pdl_enter();
   const XInvArgs& a = B ? arr[blockIdx.z] : a0;  // batched: one field per z
   if (B && (int)blockIdx.y >= a.ycount) return;
+  if (B && a.remaining && *a.remaining == 0) return;  // the member's step budget is spent
   extern __shared__ __align__(16) unsigned char smraw[];
   xinv_body<T, NX, E, MODE>(a, blockIdx.x, blockIdx.y, blockDim.x, twv, smraw);
 }
@@ -223,6 +225,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_xinv(const __grid_constant__
 // ---------------------------------------------------------------- x forward
 struct XFwdArgs {
   Geo geo;
+  const int* remaining; // batched launches: the member's step budget (0: skip the pass); nullptr: no budget
   int ycount;           // batched launches: blocks with blockIdx.y >= ycount have no work
   int rows;             // rows processed
   const int* rows_dev;  // if set, overrides rows
@@ -405,6 +408,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_xfwd(const __grid_constant__
   pdl_enter();
   const XFwdArgs& a = B ? arr[blockIdx.z] : a0;
   if (B && (int)blockIdx.y >= a.ycount) return;
+  if (B && a.remaining && *a.remaining == 0) return;  // the member's step budget is spent
   extern __shared__ __align__(16) unsigned char smraw[];
   xfwd_body<T, NX, E, MODE>(a, blockIdx.x, blockIdx.y, blockDim.x, twv, smraw);
 }
@@ -488,6 +492,7 @@ struct YJob {
 
 struct YInvArgs {
   Geo geo;
+  const int* remaining; // batched launches: the member's step budget (0: skip the pass); nullptr: no budget
   int ycount;           // batched launches: blocks with blockIdx.y >= ycount have no work
   int lp;            // line pitch in shared memory (complex elements)
   const void* z;     // Z arrays (T2), stride (h+1)*nx
@@ -664,12 +669,14 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yinv(const __grid_constant__
   pdl_enter();
   const YInvArgs& a = B ? arr[blockIdx.z] : a0;
   if (B && (int)blockIdx.y >= a.ycount) return;
+  if (B && a.remaining && *a.remaining == 0) return;  // the member's step budget is spent
   extern __shared__ __align__(16) unsigned char smraw[];
   yinv_body<T, H, E, MODE>(a, blockIdx.x, blockIdx.y, blockDim.x, twv, twyv, smraw);
 }
 
 struct YFwdArgs {
   Geo geo;
+  const int* remaining; // batched launches: the member's step budget (0: skip the pass); nullptr: no budget
   int ycount;           // batched launches: blocks with blockIdx.y >= ycount have no work
   int lp;
   const void* phys;   // physical arrays (T), stride nx*ny
@@ -814,6 +821,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 2) k_yfwd(const __grid_constant__
   pdl_enter();
   const YFwdArgs& a = B ? arr[blockIdx.z] : a0;
   if (B && (int)blockIdx.y >= a.ycount) return;
+  if (B && a.remaining && *a.remaining == 0) return;  // the member's step budget is spent
   extern __shared__ __align__(16) unsigned char smraw[];
   yfwd_body<T, H, E, MODE>(a, blockIdx.x, blockIdx.y, blockDim.x, twv, twyv, smraw);
 }
@@ -834,6 +842,7 @@ struct StepEndArgs {
   int hist_cap;
   long long* bad_step;  // first step whose energy was not finite (-1: none)
   int* any_bad;         // ensemble-wide word set with bad_step (nullptr outside ensembles)
+  int* remaining;       // the member's step budget, counted down here (nullptr: none)
 };
 
 __device__ __forceinline__ void step_end_body(const StepEndArgs& a, int nthreads) {
@@ -860,6 +869,7 @@ __device__ __forceinline__ void step_end_body(const StepEndArgs& a, int nthreads
   }
   *a.tdev = *a.tdev + a.dt;
   *a.stepdev = st + 1;
+  if (a.remaining && *a.remaining > 0) *a.remaining = *a.remaining - 1;
 }
 
 }  // namespace hos

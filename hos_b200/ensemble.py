@@ -8,14 +8,15 @@ include/hos_gpu.h):
   persistent kernel; its resident blocks take work items (blocks of one pass
   of one member) from a device list in order and wait, with a bounded wait,
   for the member's earlier passes.  Grids of 64..2048 points per direction,
-  default kernel shapes.  Members can be given step budgets: a member stops
-  after its own number of steps while the others go on.
+  default kernel shapes.
 * ``"classes"``: members that share grid, precision and scheme form a size
   class; every pass of the RK step is one kernel launch over all members of
   the class, and a whole step of all classes is one CUDA graph with the
   classes on parallel streams.
 
-Either way each member advances exactly as ``field.step(dt)`` would; the
+In both modes members can be given step budgets: a member stops after its
+own number of steps while the others go on.  Either way each member
+advances exactly as ``field.step(dt)`` would; the
 reference advances one field per process and has no counterpart.
 """
 from __future__ import annotations
@@ -42,8 +43,8 @@ class HosEnsemble:
         self._h = h
 
     def set_steps(self, steps):
-        """Persistent mode: each member takes steps[i] more steps and then
-        stops (-1: no limit), whatever number of launches follows."""
+        """Each member takes steps[i] more steps and then stops (-1: no
+        limit), whatever number of steps is launched (either mode)."""
         arr = (ctypes.c_int * len(self.fields))(*[int(s) for s in steps])
         _lib.check(self._lib.hos_ensemble_set_steps(self._h, arr))
 

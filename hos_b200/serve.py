@@ -9,9 +9,9 @@ number of RK4 steps).  The server
   request that does not fit does not block smaller ones behind it;
 * keeps each admitted field's FP64 spectral state resident on the device
   (one ``HosField`` per request) until it finishes;
-* advances all active fields together as one persistent ``HosEnsemble``
-  (one kernel launch per RK step for every member, each member with its own
-  step budget on the device) in chunks of about ``chunk_seconds``; requests
+* advances all active fields together as one ``HosEnsemble`` (each member
+  with its own step budget on the device) in chunks of about
+  ``chunk_seconds``; requests
   that arrive meanwhile are admitted while the chunk runs and join at its
   end, and a request stops at exactly its own number of steps, inside a
   chunk, and leaves at the chunk's end (its slot and memory are freed);
@@ -118,10 +118,15 @@ def jonswap_device(n, kp, steepness, seed, depth=None, gamma=3.3, spread_s=10.0,
 
 class DeviceBackend:
     """The server's device side: one ``HosField`` per admitted request, one
-    persistent ``HosEnsemble`` over the active fields with a step budget per
-    member.  The request loop in ``Server`` only calls these methods, so that
-    its queueing, admission, cancellation and failure handling can be
-    exercised without a GPU."""
+    ``HosEnsemble`` over the active fields with a step budget per member
+    (``mode``: "classes", one launch per pass per size class in a CUDA graph
+    per step, the faster on B200 for this mix of grids; or "persistent", one
+    launch per step).  The request loop in ``Server`` only calls these
+    methods, so that its queueing, admission, cancellation and failure
+    handling can be exercised without a GPU."""
+
+    def __init__(self, mode="classes"):
+        self.mode = mode
 
     def footprint(self, r):
         return HosField.footprint_bytes(r.n, r.n, r.order, r.precision)
@@ -143,9 +148,9 @@ class DeviceBackend:
         return f, tp / 50
 
     def group(self, fields, dts, budgets):
-        """One persistent ensemble over the fields; member i takes at most
-        budgets[i] more steps, whatever number of steps is launched."""
-        g = HosEnsemble(fields, dts, mode="persistent")
+        """One ensemble over the fields; member i takes at most budgets[i]
+        more steps, whatever number of steps is launched."""
+        g = HosEnsemble(fields, dts, mode=self.mode)
         try:
             g.set_steps(budgets)
         except Exception:
@@ -195,10 +200,9 @@ class Server:
     steps over the measured rate) stays under ``max_inflight_s`` seconds;
     a request that does not fit does not block smaller ones behind it.
 
-    The loop runs the active fields in chunks: one launch of the persistent
-    ensemble per step, ``chunk`` steps at most and about ``chunk_seconds`` of
-    device time (sized from the previous chunk).  Every member has a step
-    budget on the device, so a request stops at exactly its own number of
+    The loop runs the active fields in chunks of ensemble steps, ``chunk``
+    steps at most and about ``chunk_seconds`` of device time (sized from the
+    previous chunk).  Every member has a step budget on the device, so a request stops at exactly its own number of
     steps inside a chunk and the others go on.  While a chunk runs, the loop
     admits arrived requests (creates their fields and uploads their initial
     seas); they join at the chunk's end, when the work list is re-planned.

@@ -210,7 +210,7 @@ int hos_ensemble_create(const hos_handle* members, const double* dt, int n, hos_
  * the reference (time_schemes_par.c:28-121 advances one field per process). */
 enum { HOS_ENS_CLASSES = 0, HOS_ENS_PERSISTENT = 1 };
 int hos_ensemble_create_ex(const hos_handle* members, const double* dt, int n, int mode, hos_ensemble* out);
-/* Persistent ensembles: per-member step budgets.  steps[i] >= 0 lets member
+/* Per-member step budgets (either mode).  steps[i] >= 0 lets member
  * i take that many more steps, after which its work items are skipped (its
  * state and time stay as they are) until a new budget is set; -1 (the value
  * after create) sets no limit.  get_remaining reads what is left (after the

@@ -122,14 +122,15 @@ def test_persistent_ensemble_wait_runs_out_and_recovers():
         f.close()
 
 
-def test_persistent_ensemble_step_budgets():
+@pytest.mark.parametrize("mode", ["persistent", "classes"])
+def test_ensemble_step_budgets(mode):
     """Members stop after their own number of steps inside a run of
     launches: each ends bitwise as hos_step after that many steps."""
     specs = [(128, 3, "fp32", None, 8.0, 21), (256, 5, "fp32", 0.4, 12.0, 22), (64, 4, "fp32", None, 4.0, 23)]
     budgets = [2, 5, 0]
     solo = [solo_runs([s], b)[0] for s, b in zip(specs, budgets)]
     fields, dts = zip(*[make(s) for s in specs])
-    with HosEnsemble(fields, dts, mode="persistent") as ens:
+    with HosEnsemble(fields, dts, mode=mode) as ens:
         ens.set_steps(budgets)
         ens.step(7)
         ens.sync()
