@@ -390,9 +390,6 @@ struct hos_ctx {
   void* zbuf = nullptr;
   void* phys = nullptr;
   double2* ustage = nullptr;
-  void* zlev = nullptr;      // Z / V arrays of the Taylor levels (M of them), apart from the stage's
-  cudaStream_t st2 = nullptr;  // second stream of a step graph: the stage's off-critical-path transforms
-  cudaEvent_t ev[16] = {};     // fork / join events of the step graph
   double2* ustg = nullptr;  // stage input of the current RK stage
   double2* zvbuf = nullptr; // Zvel outputs / operator scratch (allocated on first use)
   double* hpart = nullptr;  // Hamiltonian row partials (allocated on first use)
@@ -572,8 +569,7 @@ size_t compute_bytes(const hos_params* p, int nst) {
   size_t b = 0;
   b += 2 * fsz * 16;                                 // u
   b += (size_t)nst * 2 * fsz * 16;                   // k
-  b += (size_t)(4 + M) * fsz * cs;                   // Z / V scratch of a stage
-  b += (size_t)M * fsz * cs;                         // Z / V scratch of the Taylor levels
+  b += (size_t)(4 + M) * fsz * cs;                   // Z / V scratch
   b += (size_t)(5 + M * (M + 1) / 2 + L) * psz * rs; // physical fields
   b += 2 * fsz * 16 + fsz * 16 + 2 * psz * 8;        // boundary scratch (FP64)
   b += 2 * fsz * 16;                                 // stage input
@@ -619,10 +615,6 @@ struct PassRec {
   int gx = 1, gy = 1;  // grid (x: rows or x-row groups, y: outputs)
   int log_kind = 0;    // PassKind for the per-pass profile
   double bytes = 0.0;  // algorithmic bytes of the launch
-  // split stages (one field's step graph): the stream of the launch (0 the
-  // handle's, 1 its second one), an event it waits for first and one it
-  // records after (indices into hos_ctx::ev, -1 none)
-  int stream = 0, wait_ev = -1, signal_ev = -1;
   XInvArgs xi{};
   XFwdArgs xf{};
   YInvArgs yi{};
@@ -646,17 +638,13 @@ bool strip_plain() {
 // are written there (4 consecutive FP64 fields) instead of the RHS.
 // act_rows is only used for the byte counts of the profile.
 void build_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, double2* kout, const double* tsrc,
-                 const int* rows_dev, double2* zvel_out, int act_rows, std::vector<PassRec>& out, bool split = false) {
+                 const int* rows_dev, double2* zvel_out, int act_rows, std::vector<PassRec>& out) {
   const PassCfg& g = c->cfg;
   const int M = c->M, L = c->L;
   const size_t fsz = c->fsz;
   const size_t cs = c->prec ? sizeof(float2) : sizeof(double2);
   const size_t rs = c->prec ? sizeof(float) : sizeof(double);
   char* zb = reinterpret_cast<char*>(c->zbuf);
-  // the levels' V and Z arrays: apart from the stage's when the stage is
-  // split (its Z arrays are still being read beside the levels), else the
-  // stage's own
-  char* zl = reinterpret_cast<char*>(split ? c->zlev : c->zbuf);
   const double act = (double)act_rows;
   const double nxd = (double)c->nx, psz = (double)c->psz, fszd = (double)fsz, my = (double)c->geo.my;
 
@@ -690,29 +678,7 @@ void build_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, doub
   r1.slot = 0;
   r1.log_kind = P_XINV_STAGE;
   r1.bytes = act * nxd * (16.0 * 2 * (1 + nk) + (double)cs * (4 + M));
-  if (split) {
-    // eta and d_z phi (outputs 0 and 4) lead the Taylor levels; the others
-    // go on the second stream, which starts once these are written (the
-    // stage input of eta, written with output 0, is also read there)
-    PassRec a = r1, b = r1;
-    a.xi.omap_n = 2;
-    a.xi.omap[0] = 0;
-    a.xi.omap[1] = 4;
-    a.gy = a.xi.ycount = 2;
-    a.signal_ev = 0;
-    int nb = 0;
-    for (int o = 0; o < 4 + M; o++)
-      if (o != 0 && o != 4) b.xi.omap[nb++] = (signed char)o;
-    b.xi.omap_n = nb;
-    b.gy = b.xi.ycount = nb;
-    b.xi.set_ramp = 0;
-    b.stream = 1;
-    b.wait_ev = 0;
-    out.push_back(a);
-    out.push_back(b);
-  } else {
-    out.push_back(r1);
-  }
+  out.push_back(r1);
 
   PassRec r2;
   r2.kind = L_YINV;
@@ -738,25 +704,7 @@ void build_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, doub
   r2.slot = 1;
   r2.log_kind = P_YINV_STAGE;
   r2.bytes = act * nxd * (double)cs * (4 + M) + psz * (double)rs * (5 + M);
-  if (split) {
-    // eta and d_z phi^(1) on the handle's stream (the first level needs
-    // them); on the second stream d_z^j phi^(1) (j >= 2, needed by level
-    // j-1, event j-1) and the x/y derivatives (needed by the RHS, event M)
-    auto sub = [&](std::initializer_list<YJob> jl, int strm, int sig) {
-      PassRec q = r2;
-      int k = 0;
-      for (const YJob& jb : jl) q.yi.jobs[k++] = jb;
-      q.gy = q.yi.ycount = k;
-      q.stream = strm;
-      q.signal_ev = sig;
-      out.push_back(q);
-    };
-    sub({YJob{0, 0, c->ETA()}, YJob{4, 0, c->D(1, 1)}}, 0, -1);
-    for (int j = 2; j <= M; j++) sub({YJob{4 + j - 1, 0, c->D(1, j)}}, 1, j - 1);
-    sub({YJob{0, 1, c->ETAY()}, YJob{1, 0, c->ETAX()}, YJob{2, 1, c->PHIY()}, YJob{3, 0, c->PHIX()}}, 1, M);
-  } else {
-    out.push_back(r2);
-  }
+  out.push_back(r2);
 
   for (int n = 1; n <= L; n++) {
     const bool fused_in = c->cfg.ec.fuse && n >= 2;  // this level's y-forward ran inside level n-1's y-inverse
@@ -774,7 +722,7 @@ void build_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, doub
     fa.eta = c->ETA();
     fa.nterms = n;
     for (int p = 1; p <= n; p++) fa.t_in[p - 1] = c->D(n - p + 1, p);  // power p: m = n - p
-    fa.vout = zl;
+    fa.vout = zb;
     fa.rows_out = c->h + 1;
     r3.slot = 2 + 3 * (n - 1);
     r3.log_kind = P_YFWD_LEVEL;
@@ -794,8 +742,8 @@ void build_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, doub
     xf.ndz = M - n;
     xf.opb = opb;
     xf.rows = c->h + 1;
-    xf.vin0 = zl;
-    xf.zout = zl + fsz * cs;
+    xf.vin0 = zb;
+    xf.zout = zb + fsz * cs;
     r4.slot = 3 + 3 * (n - 1);
     r4.log_kind = P_XFWD_LEVEL;
     r4.bytes = fszd * (double)cs * (1 + M - n);
@@ -808,7 +756,7 @@ void build_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, doub
     YInvArgs& yl = r5.yi;
     yl.geo = c->geo;
     yl.lp = g.yi.lp;
-    yl.z = zl;
+    yl.z = c->zbuf;
     yl.rows_in = c->h + 1;
     yl.phys = c->phys;
     yl.plain_strip = strip_plain();
@@ -830,11 +778,10 @@ void build_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, doub
       yl.fuse_next = 1;
       yl.nx_terms = n + 1;
       for (int p = 2; p <= n + 1; p++) yl.nx_in[p - 1] = c->D(n + 2 - p, p);
-      yl.vout = zl;
+      yl.vout = zb;
       yl.store_job0 = 0;
       r5.bytes += psz * (double)rs * (n - 1) + fszd * (double)cs;
     }
-    if (split) r5.wait_ev = n;  // W_n and P_(n+1) read d_z^(n+1) phi^(1)
     out.push_back(r5);
   }
 
@@ -898,7 +845,6 @@ void build_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, doub
   ff.rows_out = c->geo.my;
   r6.slot = 100;
   r6.log_kind = P_YFWD_RHS;
-  if (split) r6.wait_ev = M;  // the second stream's last transforms
   r6.bytes = psz * (double)rs * (5 + L) + 2.0 * my * nxd * (double)cs;
   out.push_back(r6);
 
@@ -966,7 +912,7 @@ void launch_pdl(void (*kernel)(K...), dim3 grid, unsigned threads, size_t smem, 
 }
 
 // Launches one pass of one field with its arguments by value.
-void launch_single(hos_ctx* c, const PassRec& r, cudaStream_t st) {
+void launch_single(hos_ctx* c, const PassRec& r) {
   const PassCfg& g = c->cfg;
   const dim3 grid(r.gx, r.gy);
   const XInvArgs* nxi = nullptr;
@@ -977,46 +923,24 @@ void launch_single(hos_ctx* c, const PassRec& r, cudaStream_t st) {
   const void* twh = g.twh;
   const void* twy = g.twy;
   switch (r.kind) {
-    case L_XINV: launch_pdl(g.xinv[r.mode], grid, g.xi.threads, g.xi.smem, st, r.xi, nxi, twx); break;
-    case L_XFWD: launch_pdl(g.xfwd[r.mode], grid, g.xf.threads, g.xf.smem, st, r.xf, nxf, twx); break;
+    case L_XINV: launch_pdl(g.xinv[r.mode], grid, g.xi.threads, g.xi.smem, c->st, r.xi, nxi, twx); break;
+    case L_XFWD: launch_pdl(g.xfwd[r.mode], grid, g.xf.threads, g.xf.smem, c->st, r.xf, nxf, twx); break;
     case L_YINV: {
       const KindCfg& k = r.mode == YI_JOBS ? g.ys : g.yi;
-      launch_pdl(g.yinv[r.mode], grid, k.threads, k.smem, st, r.yi, nyi, twh, twy);
+      launch_pdl(g.yinv[r.mode], grid, k.threads, k.smem, c->st, r.yi, nyi, twh, twy);
       break;
     }
-    default: launch_pdl(g.yfwd[r.mode], grid, g.yf.threads, g.yf.smem, st, r.yf, nyf, twh, twy); break;
+    default: launch_pdl(g.yfwd[r.mode], grid, g.yf.threads, g.yf.smem, c->st, r.yf, nyf, twh, twy); break;
   }
 }
 
-// Split stages for one field's RK steps (HOS_SPLIT=1 in the environment):
-// the transforms the Taylor levels do not wait for (most of the stage's
-// y-inverse jobs and x-inverse outputs) run on a second stream beside the
-// level chain, joined by events where their results are read.  The launches
-// and their arithmetic are those of the unsplit stage, so the results are
-// bitwise the same.  Off by default: measured on B200 at 1024^2, M = 5 it
-// is 2.5 % faster in FP64 and 3 % slower in FP32 (the joins cost the
-// programmatic launch overlap of the passes after them, and the side
-// stream's blocks take issue slots from the latency-bound level passes).
-bool split_enabled() {
-  static const bool on = [] {
-    const char* e = getenv("HOS_SPLIT");
-    return e && e[0] == '1';
-  }();
-  return on;
-}
-
-// Enqueues one RK stage (see build_stage) on the handle's stream (and, when
-// split, its second stream, joined back before the stage ends).
+// Enqueues one RK stage (see build_stage) on the handle's stream.
 int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, double2* kout, const double* tsrc,
-                  const int* rows_dev, PassLog* lg = nullptr, double2* zvel_out = nullptr, bool split = false) {
+                  const int* rows_dev, PassLog* lg = nullptr, double2* zvel_out = nullptr) {
   std::vector<PassRec> recs;
-  split = split && !lg && !zvel_out;  // the per-pass profile times one stream
-  build_stage(c, s, dt, rhs_only, uin, kout, tsrc, rows_dev, zvel_out, lg ? lg->act_rows : 0, recs, split);
+  build_stage(c, s, dt, rhs_only, uin, kout, tsrc, rows_dev, zvel_out, lg ? lg->act_rows : 0, recs);
   for (const PassRec& r : recs) {
-    cudaStream_t st = r.stream ? c->st2 : c->st;
-    if (r.wait_ev >= 0) cudaStreamWaitEvent(st, c->ev[r.wait_ev], 0);
-    launch_single(c, r, st);
-    if (r.signal_ev >= 0) cudaEventRecord(c->ev[r.signal_ev], st);
+    launch_single(c, r);
     log_pass(c, lg, r.log_kind, r.bytes);
   }
   return HOS_OK;
@@ -1024,8 +948,7 @@ int enqueue_stage(hos_ctx* c, int s, double dt, bool rhs_only, double2* uin, dou
 
 int enqueue_step(hos_ctx* c, double dt) {
   for (int s = 0; s < c->nst; s++) {
-    int rc = enqueue_stage(c, s, dt, false, c->u, c->k + (size_t)s * 2 * c->fsz, c->tdev, c->actdev, nullptr,
-                           nullptr, split_enabled());
+    int rc = enqueue_stage(c, s, dt, false, c->u, c->k + (size_t)s * 2 * c->fsz, c->tdev, c->actdev);
     if (rc) return rc;
   }
   const double* hp = c->ham_part;
@@ -1115,14 +1038,11 @@ void release(hos_ctx* c) {
   if (!c) return;
   if (c->gexec) cudaGraphExecDestroy(c->gexec);
   if (c->graph) cudaGraphDestroy(c->graph);
-  void* ptrs[] = {c->bad_step, c->u,    c->k,    c->zbuf,    c->zlev,  c->phys,   c->ustage, c->ustg, c->zplain,   c->pplain,
+  void* ptrs[] = {c->bad_step, c->u,    c->k,    c->zbuf,    c->phys,   c->ustage, c->ustg, c->zplain,   c->pplain,
                   c->tdev, c->trhs, c->rdev,    c->stepdev, c->actdev, c->flagdev, c->ham_part,
                   c->ham_hist, c->t_hist, c->zvbuf, c->hpart, c->hpart_err, c->tw[0][0], c->tw[0][1], c->tw[0][2], c->tw[1][0], c->tw[1][1], c->tw[1][2]};
   for (void* p : ptrs)
     if (p) cudaFree(p);
-  for (cudaEvent_t e : c->ev)
-    if (e) cudaEventDestroy(e);
-  if (c->st2) cudaStreamDestroy(c->st2);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
 }
@@ -1644,11 +1564,8 @@ int hos_create(const hos_params* p, hos_handle* out) {
   const size_t rs = c->prec ? sizeof(float) : sizeof(double);
   int rc = HOS_OK;
   cudaError_t e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking);
-  for (cudaEvent_t& ev : c->ev)
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
   if (e != cudaSuccess) {
-    release(c);
+    delete c;
     return fail(HOS_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
   }
 #define HOS_AL(ptr, bytes)          \
@@ -1662,7 +1579,6 @@ int hos_create(const hos_params* p, hos_handle* out) {
   HOS_AL(c->u, 2 * c->fsz * sizeof(double2));
   HOS_AL(c->k, (size_t)c->nst * 2 * c->fsz * sizeof(double2));
   HOS_AL(c->zbuf, (size_t)c->nz * c->fsz * cs);
-  HOS_AL(c->zlev, (size_t)c->M * c->fsz * cs);
   HOS_AL(c->phys, (size_t)c->nphys * c->psz * rs);
   HOS_AL(c->ustage, 2 * c->fsz * sizeof(double2));
   HOS_AL(c->ustg, 2 * c->fsz * sizeof(double2));

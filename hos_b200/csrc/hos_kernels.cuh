@@ -126,8 +126,6 @@ struct XInvArgs {
   const double2* u;     // STAGE: packed state [2][h+1][nx]; PLAIN: one field
   const double2* kp[MAX_STAGES];  // earlier stage derivatives
   double coef[MAX_STAGES];        // dt*b[s][p]
-  int omap_n;                     // STAGE: 0, or the number of outputs listed in omap
-  signed char omap[MAX_JOBS];     // STAGE: output of block row by is omap[by] (a subset of the outputs)
   int nk;
   void* z;              // output complex arrays (T2), stride (h+1)*nx; output o = blockIdx.y
   double2* ustg;        // STAGE: the stage input is also stored here ([2][h+1][nx], rows < rows)
@@ -160,7 +158,7 @@ __device__ __forceinline__ void xinv_body(const XInvArgs& a, int bx, int by, int
   const int rows = a.rows_dev ? *a.rows_dev : a.rows;
   const Geo& geo = a.geo;
   const size_t fsz = (size_t)(geo.h + 1) * NX;
-  const int o = (MODE == XI_STAGE && a.omap_n) ? (int)a.omap[by] : by;
+  const int o = by;
 
   if (MODE == XI_STAGE && a.set_ramp && bx == 0 && o == 0 && threadIdx.x == 0) {
     double r = 1.0;
