@@ -511,6 +511,73 @@ def run_configs(args):
 
 
 # ------------------------------------------------------------------ our arm
+def run_legacy(args, eta, phi, dt, calls=40):
+    """The reference's own entry point, sol_update_RK (time_schemes_par.c:28-121),
+    called as its driver calls it (main_2d_par.c:304): FP64, the caller's
+    pageable packed state advanced in place, runtime.dat appended every call.
+    Calls per second by the host clock around `calls` calls, in the default
+    mode (state copied in and out every call) and in resident mode."""
+    import ctypes
+    import math
+    import tempfile
+    import time
+
+    import numpy as np
+
+    from hos_b200 import _lib
+
+    L = _lib.load()
+    P = ctypes.c_void_p
+    L.sol_update_RK.argtypes = [P, P, ctypes.c_double, P]
+    L.fft_2d.argtypes = [P, P, P]
+    L.hos_legacy_set_nlevs.argtypes = [ctypes.c_int]
+    L.hos_legacy_set_resident.argtypes = [ctypes.c_int]
+    L.Setup_TimeScheme.argtypes = [ctypes.c_int]
+    n = args.n
+    ctypes.c_int.in_dll(L, "Nx").value = n
+    ctypes.c_int.in_dll(L, "Ny").value = n
+    for name in ("Lx", "Ly"):
+        ctypes.c_double.in_dll(L, name).value = 2 * math.pi
+    for name in ("Kx0", "Ky0", "g"):
+        ctypes.c_double.in_dll(L, name).value = 1.0
+    ctypes.c_int.in_dll(L, "rampflg").value = 0
+    al = n * (n // 2 + 1)
+    ctypes.c_ssize_t.in_dll(L, "alloc_local").value = al
+    ctypes.c_ssize_t.in_dll(L, "local_N").value = al
+    ctypes.c_ssize_t.in_dll(L, "local_Nyhpo").value = n // 2 + 1
+    ctypes.c_ssize_t.in_dll(L, "local_1_start").value = 0
+    ctypes.c_int.in_dll(L, "mpi_rank").value = 0
+    out = {}
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as tmp:
+        os.chdir(tmp)  # runtime.dat
+        try:
+            L.hos_legacy_set_nlevs(args.order - 1)
+            L.Setup_TimeScheme(2)  # RK4
+            L.rhs_hos_setup()
+            u = np.zeros((2, n // 2 + 1, n), complex)  # pageable, as fftw_alloc_complex returns
+            for k, x in enumerate((eta, phi)):
+                xp = np.zeros((n, n + 2))
+                xp[:, :n] = x
+                L.fft_2d(P(xp.ctypes.data), P(u[k].ctypes.data), None)
+            t = np.zeros(1)
+            for mode, res in (("default", 0), ("resident", 1)):
+                L.hos_legacy_set_resident(res)
+                for _ in range(3):
+                    L.sol_update_RK(P(u.ctypes.data), P(t.ctypes.data), dt, None)
+                t0 = time.perf_counter()
+                for _ in range(calls):
+                    L.sol_update_RK(P(u.ctypes.data), P(t.ctypes.data), dt, None)
+                L.hos_legacy_sync()
+                out[mode] = calls / (time.perf_counter() - t0)
+            L.hos_legacy_set_resident(0)
+            L.rhs_hos_clean()
+        finally:
+            os.chdir(cwd)
+    return {"calls_per_s": out, "calls": calls, "precision": "fp64", "order": args.order, "grid": [n, n],
+            "state_bytes_per_call": 2 * al * 16}
+
+
 def run_ours(args, rep):
     import ctypes
 
@@ -676,8 +743,10 @@ def run_ours(args, rep):
                 "sample": f"{cb['steps']} RK4 steps ({cb['seconds']:.1f} s) of the same field on the host "
                           "(Csource/2dpar hot-path sources with the single-rank FFTW-MPI shim)",
             }
+    dropin = run_legacy(args, eta, phi, dt)
     # the figures the configurations are judged on, last so that a reader of
     # the line's tail sees them
+    line["dropin"] = dropin
     line["fp64"] = {"value": v64, "ms_per_step": timings["fp64"] / args.steps}
     line["fp32_over_fp64"] = v32 / v64
     line["accuracy"] = {
@@ -697,6 +766,7 @@ def run_ours(args, rep):
         "energy_err_rel": ham_err,
         "step_roofline_frac": round(line["step_roofline"]["achieved_gbs"] / peak, 4),
         "dominant_pass_frac": round(achieved / peak, 4),
+        "dropin_sol_update_RK_fp64_calls_per_s": {k: round(v, 1) for k, v in dropin["calls_per_s"].items()},
     }
     if "ensemble" in line:
         e = line["ensemble"]

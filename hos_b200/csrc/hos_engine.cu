@@ -32,6 +32,7 @@
 #include "hos_gpu.h"
 #include "hos_persist.h"
 #include "hos_registry.h"
+#include "hos_stage.h"
 
 namespace hos {
 XInvFn lookup_xinv_64(int mode, int n, int e, bool batch);
@@ -1694,7 +1695,7 @@ void* hos_stream(hos_handle h) { return h ? (void*)h->st : nullptr; }
 int hos_set_state_spectral(hos_handle h, const double* u, double t) {
   if (!h || !u) return fail(HOS_ERR_ARG, "null argument");
   HOS_CK(cudaMemsetAsync(h->bad_step, 0xff, sizeof(long long), h->st));
-  HOS_CK(cudaMemcpyAsync(h->u, u, 2 * h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+  HOS_CK(host_copy(h->u, u, 2 * h->fsz * sizeof(double2), h->st));
   HOS_CK(cudaMemcpyAsync(h->tdev, &t, sizeof(double), cudaMemcpyHostToDevice, h->st));
   refresh_active_rows(h, h->u, h->actdev);
   HOS_CK(cudaGetLastError());
@@ -1704,7 +1705,7 @@ int hos_set_state_spectral(hos_handle h, const double* u, double t) {
 
 int hos_get_state_spectral(hos_handle h, double* u, double* t) {
   if (!h || !u) return fail(HOS_ERR_ARG, "null argument");
-  HOS_CK(cudaMemcpyAsync(u, h->u, 2 * h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+  HOS_CK(host_copy(u, h->u, 2 * h->fsz * sizeof(double2), h->st));
   double tt = 0;
   HOS_CK(cudaMemcpyAsync(&tt, h->tdev, sizeof(double), cudaMemcpyDeviceToHost, h->st));
   HOS_CK(cudaStreamSynchronize(h->st));
@@ -1715,8 +1716,8 @@ int hos_get_state_spectral(hos_handle h, double* u, double* t) {
 int hos_set_state_physical(hos_handle h, const double* eta, const double* phi, double t) {
   if (!h || !eta || !phi) return fail(HOS_ERR_ARG, "null argument");
   HOS_CK(cudaMemsetAsync(h->bad_step, 0xff, sizeof(long long), h->st));
-  HOS_CK(cudaMemcpyAsync(h->pplain, eta, h->psz * sizeof(double), cudaMemcpyDefault, h->st));
-  HOS_CK(cudaMemcpyAsync(h->pplain + h->psz, phi, h->psz * sizeof(double), cudaMemcpyDefault, h->st));
+  HOS_CK(host_copy(h->pplain, eta, h->psz * sizeof(double), h->st));
+  HOS_CK(host_copy(h->pplain + h->psz, phi, h->psz * sizeof(double), h->st));
   enqueue_r2c(h, h->pplain, h->u, 1);
   enqueue_r2c(h, h->pplain + h->psz, h->u + h->fsz, 1);
   HOS_CK(cudaMemcpyAsync(h->tdev, &t, sizeof(double), cudaMemcpyHostToDevice, h->st));
@@ -1731,8 +1732,8 @@ int hos_get_state_physical(hos_handle h, double* eta, double* phi) {
   enqueue_c2r(h, h->u, h->pplain);
   enqueue_c2r(h, h->u + h->fsz, h->pplain + h->psz);
   HOS_CK(cudaGetLastError());
-  HOS_CK(cudaMemcpyAsync(eta, h->pplain, h->psz * sizeof(double), cudaMemcpyDefault, h->st));
-  HOS_CK(cudaMemcpyAsync(phi, h->pplain + h->psz, h->psz * sizeof(double), cudaMemcpyDefault, h->st));
+  HOS_CK(host_copy(eta, h->pplain, h->psz * sizeof(double), h->st));
+  HOS_CK(host_copy(phi, h->pplain + h->psz, h->psz * sizeof(double), h->st));
   HOS_CK(cudaStreamSynchronize(h->st));
   return HOS_OK;
 }
@@ -1842,16 +1843,22 @@ int hos_energy_history(hos_handle h, double* t_out, double* ham_out, int max, in
     first = steps - max;
     n = max;
   }
-  std::vector<double> th(HIST_CAP), hh(HIST_CAP);
-  if (n > 0) {
-    HOS_CK(cudaMemcpy(th.data(), h->t_hist, HIST_CAP * sizeof(double), cudaMemcpyDeviceToHost));
-    HOS_CK(cudaMemcpy(hh.data(), h->ham_hist, HIST_CAP * sizeof(double), cudaMemcpyDeviceToHost));
+  // the n records are consecutive slots of the ring (at most two runs);
+  // only those are read back
+  std::vector<double> th((size_t)n), hh((size_t)n);
+  for (long long i = 0; i < n;) {
+    const long long slot = (first + i) % HIST_CAP;
+    const long long run = std::min(n - i, (long long)HIST_CAP - slot);
+    HOS_CK(cudaMemcpyAsync(th.data() + i, h->t_hist + slot, (size_t)run * sizeof(double), cudaMemcpyDeviceToHost,
+                           h->st));
+    HOS_CK(cudaMemcpyAsync(hh.data() + i, h->ham_hist + slot, (size_t)run * sizeof(double), cudaMemcpyDeviceToHost,
+                           h->st));
+    i += run;
   }
+  if (n > 0) HOS_CK(cudaStreamSynchronize(h->st));
   for (long long i = 0; i < n; i++) {
-    const long long s = first + i;
-    const size_t slot = (size_t)(s % HIST_CAP);
-    if (t_out) t_out[i] = th[slot];
-    if (ham_out) ham_out[i] = hh[slot];
+    if (t_out) t_out[i] = th[(size_t)i];
+    if (ham_out) ham_out[i] = hh[(size_t)i];
   }
   *count = (int)n;
   return HOS_OK;
@@ -1868,14 +1875,14 @@ int hos_clear_history(hos_handle h) {
 
 int hos_rhs(hos_handle h, const double* u, double* rhs, double t) {
   if (!h || !u || !rhs) return fail(HOS_ERR_ARG, "null argument");
-  HOS_CK(cudaMemcpyAsync(h->ustage, u, 2 * h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+  HOS_CK(host_copy(h->ustage, u, 2 * h->fsz * sizeof(double2), h->st));
   HOS_CK(cudaMemcpyAsync(h->trhs, &t, sizeof(double), cudaMemcpyHostToDevice, h->st));
   // the last stage buffer is scratch between steps; rows ky >= my stay zero
   double2* kout = h->k + (size_t)(h->nst - 1) * 2 * h->fsz;
   int rc = enqueue_stage(h, 0, 0.0, true, h->ustage, kout, h->trhs, nullptr);
   if (rc) return rc;
   HOS_CK(cudaGetLastError());
-  HOS_CK(cudaMemcpyAsync(rhs, kout, 2 * h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+  HOS_CK(host_copy(rhs, kout, 2 * h->fsz * sizeof(double2), h->st));
   HOS_CK(cudaStreamSynchronize(h->st));
   return HOS_OK;
 }
@@ -1886,14 +1893,14 @@ int hos_fft_2d_ld(hos_handle h, const double* u_phys, int ld, double* hu) {
                            h->ny * sizeof(double), h->nx, cudaMemcpyDefault, h->st));
   enqueue_r2c(h, h->pplain, h->ustage, 0);
   HOS_CK(cudaGetLastError());
-  HOS_CK(cudaMemcpyAsync(hu, h->ustage, h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+  HOS_CK(host_copy(hu, h->ustage, h->fsz * sizeof(double2), h->st));
   HOS_CK(cudaStreamSynchronize(h->st));
   return HOS_OK;
 }
 
 int hos_ifft_2d_ld(hos_handle h, const double* hu, double* u_phys, int ld) {
   if (!h || !hu || !u_phys || ld < h->ny) return fail(HOS_ERR_ARG, "bad argument");
-  HOS_CK(cudaMemcpyAsync(h->ustage, hu, h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+  HOS_CK(host_copy(h->ustage, hu, h->fsz * sizeof(double2), h->st));
   enqueue_c2r(h, h->ustage, h->pplain);
   HOS_CK(cudaGetLastError());
   HOS_CK(cudaMemcpy2DAsync(u_phys, (size_t)ld * sizeof(double), h->pplain, h->ny * sizeof(double),
@@ -1904,20 +1911,20 @@ int hos_ifft_2d_ld(hos_handle h, const double* hu, double* u_phys, int ld) {
 
 int hos_fft_2d(hos_handle h, const double* u_phys, double* hu) {
   if (!h || !u_phys || !hu) return fail(HOS_ERR_ARG, "null argument");
-  HOS_CK(cudaMemcpyAsync(h->pplain, u_phys, h->psz * sizeof(double), cudaMemcpyDefault, h->st));
+  HOS_CK(host_copy(h->pplain, u_phys, h->psz * sizeof(double), h->st));
   enqueue_r2c(h, h->pplain, h->ustage, 0);
   HOS_CK(cudaGetLastError());
-  HOS_CK(cudaMemcpyAsync(hu, h->ustage, h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+  HOS_CK(host_copy(hu, h->ustage, h->fsz * sizeof(double2), h->st));
   HOS_CK(cudaStreamSynchronize(h->st));
   return HOS_OK;
 }
 
 int hos_ifft_2d(hos_handle h, const double* hu, double* u_phys) {
   if (!h || !hu || !u_phys) return fail(HOS_ERR_ARG, "null argument");
-  HOS_CK(cudaMemcpyAsync(h->ustage, hu, h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+  HOS_CK(host_copy(h->ustage, hu, h->fsz * sizeof(double2), h->st));
   enqueue_c2r(h, h->ustage, h->pplain);
   HOS_CK(cudaGetLastError());
-  HOS_CK(cudaMemcpyAsync(u_phys, h->pplain, h->psz * sizeof(double), cudaMemcpyDefault, h->st));
+  HOS_CK(host_copy(u_phys, h->pplain, h->psz * sizeof(double), h->st));
   HOS_CK(cudaStreamSynchronize(h->st));
   return HOS_OK;
 }
@@ -1985,13 +1992,13 @@ int hos_zvel(hos_handle h, const double* u, double* wM, double* wM2, double* w2M
     int rc = dalloc(&h->zvbuf, 4 * h->fsz * sizeof(double2));
     if (rc) return rc;
   }
-  HOS_CK(cudaMemcpyAsync(h->ustage, u, 2 * h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+  HOS_CK(host_copy(h->ustage, u, 2 * h->fsz * sizeof(double2), h->st));
   int rc = enqueue_stage(h, 0, 0.0, true, h->ustage, nullptr, h->trhs, nullptr, nullptr, h->zvbuf);
   if (rc) return rc;
   HOS_CK(cudaGetLastError());
   double* outs[4] = {wM, wM2, w2M, w2M2};
   for (int q = 0; q < 4; q++)
-    HOS_CK(cudaMemcpyAsync(outs[q], h->zvbuf + (size_t)q * h->fsz, h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+    HOS_CK(host_copy(outs[q], h->zvbuf + (size_t)q * h->fsz, h->fsz * sizeof(double2), h->st));
   HOS_CK(cudaStreamSynchronize(h->st));
   return HOS_OK;
 }
@@ -2006,8 +2013,8 @@ int hos_spectral_op(hos_handle h, int op, const double* a, const double* b, doub
   double2* da = h->zvbuf;
   double2* db = h->zvbuf + h->fsz;
   double2* dout = h->zvbuf + 2 * h->fsz;
-  HOS_CK(cudaMemcpyAsync(da, a, h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
-  if (b) HOS_CK(cudaMemcpyAsync(db, b, h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+  HOS_CK(host_copy(da, a, h->fsz * sizeof(double2), h->st));
+  if (b) HOS_CK(host_copy(db, b, h->fsz * sizeof(double2), h->st));
   if (op == HOS_OP_MULT) {  // Mult, operators_par.c:210-235
     enqueue_c2r(h, da, h->pplain);
     enqueue_c2r(h, db, h->pplain + h->psz);
@@ -2017,7 +2024,7 @@ int hos_spectral_op(hos_handle h, int op, const double* a, const double* b, doub
     k_spec_op<<<296, 256, 0, h->st>>>(h->geo, op, da, db, dout);
   }
   HOS_CK(cudaGetLastError());
-  HOS_CK(cudaMemcpyAsync(out, dout, h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+  HOS_CK(host_copy(out, dout, h->fsz * sizeof(double2), h->st));
   HOS_CK(cudaStreamSynchronize(h->st));
   return HOS_OK;
 }
@@ -2034,7 +2041,7 @@ int hos_hamiltonian(hos_handle h, const double* eta, const double* eta_t, const 
   }
   const double* src[3] = {eta, eta_t, phi};
   for (int q = 0; q < 3; q++)
-    HOS_CK(cudaMemcpyAsync(h->zvbuf + (size_t)q * h->fsz, src[q], h->fsz * sizeof(double2), cudaMemcpyDefault, h->st));
+    HOS_CK(host_copy(h->zvbuf + (size_t)q * h->fsz, src[q], h->fsz * sizeof(double2), h->st));
   k_ham_rows<<<h->h + 1, 256, 0, h->st>>>(h->geo, h->zvbuf, h->zvbuf + h->fsz, h->zvbuf + 2 * h->fsz, h->hpart);
   k_sum_parts<<<1, 256, 0, h->st>>>(h->hpart, h->h + 1, h->hpart + h->h + 1);
   HOS_CK(cudaGetLastError());

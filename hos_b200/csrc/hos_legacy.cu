@@ -193,7 +193,7 @@ void sol_update_RK(double* u, double* t, double dt, char* dtflag) {
       return;
     }
   }
-  if (hos_clear_history(h) || hos_step(h, dt, 1)) {
+  if (hos_step(h, dt, 1)) {
     // the device state may be partly advanced: forget it, so that the next
     // call uploads the caller's array again instead of syncing this one over it
     L.resident = nullptr;
@@ -209,6 +209,7 @@ void sol_update_RK(double* u, double* t, double dt, char* dtflag) {
     report("sol_update_RK");
     return;
   }
+  // the newest record of the energy history is this step's stage-0 Hamiltonian
   double tt = 0.0, hh = 0.0;
   int n = 0;
   if (hos_energy_history(h, &tt, &hh, 1, &n) == HOS_OK && n == 1) Ham = hh;
