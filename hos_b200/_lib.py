@@ -81,6 +81,7 @@ _SIGNATURES = {
     "hos_create": (_I, [ctypes.POINTER(HosParams), ctypes.POINTER(_H)]),
     "hos_destroy": (_I, [_H]),
     "hos_footprint_bytes": (ctypes.c_size_t, [ctypes.POINTER(HosParams)]),
+    "hos_device_free_bytes": (ctypes.c_int, [ctypes.POINTER(ctypes.c_size_t)]),
     "hos_get_bounds": (_I, [_H, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "hos_set_state_spectral": (_I, [_H, _P, _D]),
     "hos_get_state_spectral": (_I, [_H, _P, _DP]),

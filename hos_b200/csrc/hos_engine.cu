@@ -1042,9 +1042,16 @@ void release(hos_ctx* c) {
   void* ptrs[] = {c->bad_step, c->u,    c->k,    c->zbuf,    c->phys,   c->ustage, c->ustg, c->zplain,   c->pplain,
                   c->tdev, c->trhs, c->rdev,    c->stepdev, c->actdev, c->flagdev, c->ham_part,
                   c->ham_hist, c->t_hist, c->zvbuf, c->hpart, c->hpart_err, c->tw[0][0], c->tw[0][1], c->tw[0][2], c->tw[1][0], c->tw[1][1], c->tw[1][2]};
+  // the handle's memory came from the stream-ordered pool on its stream
+  // (dalloc_on): freeing it there waits for nothing else on the device
   for (void* p : ptrs)
-    if (p) cudaFree(p);
-  if (c->st) cudaStreamDestroy(c->st);
+    if (p) {
+      if (c->st)
+        cudaFreeAsync(p, c->st);
+      else
+        cudaFree(p);
+    }
+  if (c->st) cudaStreamDestroy(c->st);  // released once its queued frees have run
   delete c;
 }
 
@@ -1077,6 +1084,58 @@ int dalloc(P** p, size_t bytes) {
     (void)cudaGetLastError();
     *p = nullptr;
     return fail(e == cudaErrorMemoryAllocation ? HOS_ERR_NOMEM : HOS_ERR_CUDA, "cudaMalloc(%zu): %s", bytes,
+                cudaGetErrorString(e));
+  }
+  return HOS_OK;
+}
+
+// Bytes the device's stream-ordered pool may keep for reuse after handles
+// release memory (HOS_POOL_KEEP_MB, default 8 GiB); above that, released
+// memory goes back to the driver at the next synchronisation.
+unsigned long long pool_keep_bytes() {
+  static const unsigned long long keep = [] {
+    const char* s = getenv("HOS_POOL_KEEP_MB");
+    return (s && *s) ? (unsigned long long)atoll(s) << 20 : 8ull << 30;
+  }();
+  return keep;
+}
+
+// Sets the release threshold of the current device's default pool once.
+void pool_setup() {
+  static std::mutex mu;
+  static std::vector<int> done;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return;
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  if (std::find(done.begin(), done.end(), dev) != done.end()) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    unsigned long long keep = pool_keep_bytes();  // the attribute is a 64-bit unsigned value
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  (void)cudaGetLastError();
+  done.push_back(dev);
+}
+
+// A handle's device memory: from the device's stream-ordered pool, ordered
+// on the handle's stream.  Releasing a handle then does not wait for the
+// whole device (cudaFree does), and a handle created next reuses the memory
+// without going to the driver.  Work on other streams may use the memory
+// once the handle's stream has been synchronised.
+template <typename P>
+int dalloc_on(P** p, size_t bytes, cudaStream_t st) {
+  if (injected_alloc_failure()) {
+    *p = nullptr;
+    return fail(HOS_ERR_NOMEM, "cudaMallocAsync(%zu): injected failure (HOS_FAIL_ALLOC_AFTER)", bytes);
+  }
+  cudaError_t e = cudaMallocAsync((void**)p, bytes ? bytes : 16, st);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    *p = nullptr;
+    return fail(e == cudaErrorMemoryAllocation ? HOS_ERR_NOMEM : HOS_ERR_CUDA, "cudaMallocAsync(%zu): %s", bytes,
                 cudaGetErrorString(e));
   }
   return HOS_OK;
@@ -1520,6 +1579,21 @@ size_t hos_footprint_bytes(const hos_params* p) {
   return compute_bytes(p, nst);
 }
 
+int hos_device_free_bytes(size_t* free_bytes) {
+  if (!free_bytes) return fail(HOS_ERR_ARG, "null argument");
+  size_t fr = 0, tot = 0;
+  HOS_CK(cudaMemGetInfo(&fr, &tot));
+  int dev = 0;
+  HOS_CK(cudaGetDevice(&dev));
+  cudaMemPool_t pool;
+  HOS_CK(cudaDeviceGetDefaultMemPool(&pool, dev));
+  unsigned long long reserved = 0, used = 0;
+  HOS_CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
+  HOS_CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used));
+  *free_bytes = fr + (size_t)(reserved > used ? reserved - used : 0);
+  return HOS_OK;
+}
+
 int hos_create(const hos_params* p, hos_handle* out) {
   if (!p || !out) return fail(HOS_ERR_ARG, "null argument");
   *out = nullptr;
@@ -1564,14 +1638,20 @@ int hos_create(const hos_params* p, hos_handle* out) {
   const size_t cs = c->prec ? sizeof(float2) : sizeof(double2);
   const size_t rs = c->prec ? sizeof(float) : sizeof(double);
   int rc = HOS_OK;
-  cudaError_t e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+  // The handle's own stream takes the greatest priority: its work (uploads,
+  // steps of one field, read-backs) is short, and a server creates and reads
+  // fields while an ensemble's long chunk occupies the device.
+  int prio_least = 0, prio_greatest = 0;
+  cudaError_t e = cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest);
+  if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&c->st, cudaStreamNonBlocking, prio_greatest);
   if (e != cudaSuccess) {
     delete c;
     return fail(HOS_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
   }
-#define HOS_AL(ptr, bytes)          \
-  do {                              \
-    rc = dalloc(&(ptr), (bytes));   \
+  pool_setup();
+#define HOS_AL(ptr, bytes)                    \
+  do {                                        \
+    rc = dalloc_on(&(ptr), (bytes), c->st);   \
     if (rc) {                       \
       release(c);                   \
       return rc;                    \
@@ -1637,7 +1717,7 @@ int hos_create(const hos_params* p, hos_handle* out) {
     return rc;
   }
   c->nparts = c->h + 1;  // one Hamiltonian partial per ky row
-  rc = dalloc(&c->ham_part, (size_t)c->nparts * sizeof(double));
+  rc = dalloc_on(&c->ham_part, (size_t)c->nparts * sizeof(double), c->st);
   if (rc) {
     release(c);
     return rc;
@@ -1650,8 +1730,11 @@ int hos_create(const hos_params* p, hos_handle* out) {
       std::vector<double2> tw = twiddle_table(lens[q]);
       std::vector<float2> tw32(lens[q]);
       for (int i = 0; i < lens[q]; i++) tw32[i] = make_float2((float)tw[i].x, (float)tw[i].y);
-      e = cudaMemcpy(c->tw[0][q], tw.data(), lens[q] * sizeof(double2), cudaMemcpyHostToDevice);
-      if (e == cudaSuccess) e = cudaMemcpy(c->tw[1][q], tw32.data(), lens[q] * sizeof(float2), cudaMemcpyHostToDevice);
+      // on the handle's stream, after its allocations (pageable sources: the
+      // copies are staged before the calls return)
+      e = cudaMemcpyAsync(c->tw[0][q], tw.data(), lens[q] * sizeof(double2), cudaMemcpyHostToDevice, c->st);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(c->tw[1][q], tw32.data(), lens[q] * sizeof(float2), cudaMemcpyHostToDevice, c->st);
     }
   }
   if (e == cudaSuccess) e = cudaMemsetAsync(c->u, 0, 2 * c->fsz * sizeof(double2), c->st);
@@ -1757,7 +1840,7 @@ int hos_step_adaptive(hos_handle h, double t_end, double* dt, double rtol, doubl
   // 5th-order weights of the pair (time_schemes_par.c:225-231); the update uses c (4th order), as the reference does
   static const double cs[7] = {35.0 / 384.0, 0.0, 500.0 / 1113.0, 125.0 / 192.0, -2187.0 / 6784.0, 11.0 / 84.0, 0.0};
   if (!h->hpart_err) {
-    int rc = dalloc(&h->hpart_err, (size_t)2 * ERR_BLOCKS * sizeof(double));
+    int rc = dalloc_on(&h->hpart_err, (size_t)2 * ERR_BLOCKS * sizeof(double), h->st);
     if (rc) return rc;
   }
   int acc = 0, rej = 0;
@@ -1989,7 +2072,7 @@ int hos_profile_stage(hos_handle h, double dt, int reps, hos_pass_stat* out, int
 int hos_zvel(hos_handle h, const double* u, double* wM, double* wM2, double* w2M, double* w2M2) {
   if (!h || !u || !wM || !wM2 || !w2M || !w2M2) return fail(HOS_ERR_ARG, "null argument");
   if (!h->zvbuf) {
-    int rc = dalloc(&h->zvbuf, 4 * h->fsz * sizeof(double2));
+    int rc = dalloc_on(&h->zvbuf, 4 * h->fsz * sizeof(double2), h->st);
     if (rc) return rc;
   }
   HOS_CK(host_copy(h->ustage, u, 2 * h->fsz * sizeof(double2), h->st));
@@ -2007,7 +2090,7 @@ int hos_spectral_op(hos_handle h, int op, const double* a, const double* b, doub
   if (!h || !a || !out || ((op == HOS_OP_SUM || op == HOS_OP_MULT) && !b)) return fail(HOS_ERR_ARG, "null argument");
   if (op < HOS_OP_DX || op > HOS_OP_MULT) return fail(HOS_ERR_ARG, "unknown operator %d", op);
   if (!h->zvbuf) {
-    int rc = dalloc(&h->zvbuf, 4 * h->fsz * sizeof(double2));
+    int rc = dalloc_on(&h->zvbuf, 4 * h->fsz * sizeof(double2), h->st);
     if (rc) return rc;
   }
   double2* da = h->zvbuf;
@@ -2032,11 +2115,11 @@ int hos_spectral_op(hos_handle h, int op, const double* a, const double* b, doub
 int hos_hamiltonian(hos_handle h, const double* eta, const double* eta_t, const double* phi, double* H) {
   if (!h || !eta || !eta_t || !phi || !H) return fail(HOS_ERR_ARG, "null argument");
   if (!h->zvbuf) {
-    int rc = dalloc(&h->zvbuf, 4 * h->fsz * sizeof(double2));
+    int rc = dalloc_on(&h->zvbuf, 4 * h->fsz * sizeof(double2), h->st);
     if (rc) return rc;
   }
   if (!h->hpart) {
-    int rc = dalloc(&h->hpart, (size_t)(h->h + 2) * sizeof(double));
+    int rc = dalloc_on(&h->hpart, (size_t)(h->h + 2) * sizeof(double), h->st);
     if (rc) return rc;
   }
   const double* src[3] = {eta, eta_t, phi};

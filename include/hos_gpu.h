@@ -88,6 +88,12 @@ int hos_destroy(hos_handle h);
 /* Device bytes a handle with these parameters allocates (admission control). */
 size_t hos_footprint_bytes(const hos_params* p);
 
+/* Device memory a new handle can take on the current device: the driver's
+ * free memory plus what the stream-ordered pool that handles allocate from
+ * holds unused (memory of destroyed handles, kept up to HOS_POOL_KEEP_MB,
+ * 8 GiB by default, for the next handles). */
+int hos_device_free_bytes(size_t* free_bytes);
+
 /* Dealias bounds in effect (mx, my) for a handle. */
 int hos_get_bounds(hos_handle h, int* mx, int* my);
 

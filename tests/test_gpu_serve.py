@@ -51,3 +51,24 @@ def test_admission_by_memory_budget():
     assert m["completed"] == 6
     # at most two fields fit at a time, so six requests need at least three ensembles
     assert m["ensemble_rebuilds"] >= 3
+
+
+def test_device_free_bytes_counts_memory_of_released_fields():
+    """Fields take their memory from a stream-ordered pool; memory a closed
+    field leaves there counts as free for the next one."""
+    import ctypes
+
+    import torch
+
+    from hos_b200 import HosField, _lib
+
+    L = _lib.load()
+    out = ctypes.c_size_t()
+    f = HosField(512, 512, order=4, precision="fp32")
+    f.close()
+    torch.cuda.synchronize()
+    assert L.hos_device_free_bytes(ctypes.byref(out)) == 0
+    assert out.value >= torch.cuda.mem_get_info()[0]
+    g = HosField(512, 512, order=4, precision="fp32")  # reuses the pool's memory
+    assert L.hos_device_free_bytes(ctypes.byref(out)) == 0 and out.value > 0
+    g.close()

@@ -199,3 +199,31 @@ def test_inflight_work_bound_keeps_the_rest_queued():
     assert m["completed"] == 4 and be.max_group == 1
     assert [r.rid for r in sorted(rs, key=lambda r: r.admitted)] == [0, 1, 2, 3]
     assert all(r.result == (r.steps,) for r in rs)
+
+
+def test_fields_created_on_the_opener_thread():
+    """The same service with fields created on a thread beside the loop."""
+    be = FakeBackend(3 * 8 * 8 * 2 + 10)
+    rs = reqs(7)
+    m = Server(chunk=4, reserve_bytes=0, backend=be, open_thread=True).run(rs, realtime=False)
+    assert m["completed"] == 7 and be.peak_held <= 3 * 8 * 8 * 2
+    for r in rs:
+        assert r.status == "done" and r.result == (r.steps,)
+    assert be.held == 0 and all(f.closed for f in be.opened)
+
+
+def test_arrivals_while_others_run_join_at_a_replan():
+    """Requests that arrive while a chunk runs are created in the chunk's
+    window and join at a later re-plan (built during the chunk before it);
+    each still gets exactly its steps."""
+    be = FakeBackend(1 << 30, on_advance=lambda b: time.sleep(0.002))
+    rs = reqs(6, steps=40)
+    for i, r in enumerate(rs):
+        r.arrival = 0.004 * i
+    m = Server(chunk=2, reserve_bytes=0, backend=be, rebuild_seconds=0.01).run(rs, realtime=True)
+    assert m["completed"] == 6 and m["ensemble_rebuilds"] >= 2
+    # re-plans are built while the chunk before them runs
+    assert m["rebuilds_prebuilt"] >= 1
+    for r in rs:
+        assert r.status == "done" and r.result == (r.steps,)
+    assert be.held == 0 and all(f.closed for f in be.opened)
