@@ -393,7 +393,10 @@ def run_serving(args, capacity_gps):
     reqs = poisson_requests(rate, args.serve_duration, seed=4)
     m = Server(keep_results=False).run(reqs, realtime=True, time_limit=args.serve_limit)
     done = [r for r in reqs if r.status == "done"]
-    seq = sequential_fp64_rate(done, {}) if done else None
+    cache = {}
+    seq = sequential_fp64_rate(done, cache) if done else None
+    done_nom = [r for r in nominal if r.status == "done"]
+    seq_nom = sequential_fp64_rate(done_nom, cache) if done_nom else None
     m.update({
         "arrival_rate_per_s": rate,
         "arrival_window_s": args.serve_duration,
@@ -409,6 +412,9 @@ def run_serving(args, capacity_gps):
             "completed": m_nom["completed"], "backlog_queued": m_nom["backlog_queued"],
             "backlog_running": m_nom["backlog_running"], "p50_s_of_completed": m_nom["p50_s"],
             "p99_s_of_completed": m_nom["p99_s"], "grid_point_steps_per_s": m_nom["grid_point_steps_per_s"],
+            "sequential_fp64_grid_point_steps_per_s": seq_nom,
+            "vs_sequential_fp64": (m_nom["grid_point_steps_per_s"] / seq_nom) if seq_nom else None,
+            "ensemble_rebuilds": m_nom["ensemble_rebuilds"], "host_seconds": m_nom["host_seconds"],
         },
     })
     return m
@@ -783,7 +789,8 @@ def run_ours(args, rep):
                                                   "grid_point_steps_per_s", "vs_sequential_fp64")}
         nm = sv.get("nominal_stream", {})
         summ["serving_nominal_200_per_s"] = {k: nm.get(k) for k in ("completed", "backlog_queued", "backlog_running",
-                                                                     "p50_s_of_completed", "p99_s_of_completed")}
+                                                                     "p50_s_of_completed", "p99_s_of_completed",
+                                                                     "grid_point_steps_per_s", "vs_sequential_fp64")}
     line["summary"] = summ
     for fl in fields.values():
         fl.close()

@@ -246,8 +246,8 @@ class Server:
     footprint exceeds what the device offers with the server holding
     nothing)."""
 
-    def __init__(self, chunk=64, chunk_seconds=0.05, max_slots=4096, reserve_bytes=2 << 30, hbm_budget_bytes=None,
-                 keep_results=True, backend=None, max_inflight_s=4.0, rebuild_seconds=0.25,
+    def __init__(self, chunk=64, chunk_seconds=0.1, max_slots=4096, reserve_bytes=2 << 30, hbm_budget_bytes=None,
+                 keep_results=True, backend=None, max_inflight_s=4.0, rebuild_seconds=0.5,
                  open_thread=False, prebuild=True):
         self.chunk = int(chunk)
         self.chunk_seconds = float(chunk_seconds)
@@ -588,10 +588,10 @@ class Server:
                 # when a re-plan is due after this chunk, build it now, while
                 # the chunk runs: the members that keep running (with the
                 # budgets they will have) and the fields opened so far
-                tnow = time.perf_counter() - t0
+                t_end = time.perf_counter() - t0 + (step_s * steps if step_s else 0.0)  # when the chunk should end
                 leaving = any(a[3] <= steps for a in active)
                 if (not dirty and (staged or leaving) and self.prebuild
-                        and (last_build is None or tnow - last_build >= self.rebuild_seconds)):
+                        and (last_build is None or t_end - last_build >= self.rebuild_seconds)):
                     keep = [a for a in active if a[3] > steps]
                     new_fields = list(staged)
                     if keep or new_fields:
