@@ -343,7 +343,8 @@ def run_ensemble(args, rep):
 def sequential_fp64_rate(reqs, cache):
     """Grid-point-steps/s of the requests run one after another in plain
     FP64 (each (n, M, depth?) kind timed once on 20 steps, weighted by the
-    requests' work)."""
+    work the server did on each request: the steps it took, all of them for
+    a completed request)."""
     import torch
 
     from hos_b200 import HosField
@@ -367,8 +368,8 @@ def sequential_fp64_rate(reqs, cache):
             g.sync()
             cache[key] = e0.elapsed_time(e1) / 1e3 / 20
             g.close()
-        work += r.n * r.n * r.steps
-        secs += cache[key] * r.steps
+        work += r.n * r.n * r.steps_done
+        secs += cache[key] * r.steps_done
     return work / secs if secs > 0 else None
 
 
@@ -395,8 +396,10 @@ def run_serving(args, capacity_gps):
     done = [r for r in reqs if r.status == "done"]
     cache = {}
     seq = sequential_fp64_rate(done, cache) if done else None
-    done_nom = [r for r in nominal if r.status == "done"]
-    seq_nom = sequential_fp64_rate(done_nom, cache) if done_nom else None
+    # the nominal stream ends at its time limit with requests still running:
+    # the comparison covers every step the server took, finished or not
+    worked = [r for r in nominal if r.steps_done > 0]
+    seq_nom = sequential_fp64_rate(worked, cache) if worked else None
     m.update({
         "arrival_rate_per_s": rate,
         "arrival_window_s": args.serve_duration,

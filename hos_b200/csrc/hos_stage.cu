@@ -4,13 +4,20 @@
 // buffers with one host thread; the reference's driver passes its whole
 // packed state (two complex fields, 16.8 MB at 1024^2) this way twice per
 // sol_update_RK call.  Here the host side of the staging is split over
-// several threads and overlapped with the copy engine, chunk by chunk.
+// several threads and overlapped with the copy engine: host to device, the
+// threads fill one half of the pinned buffer while the copy engine empties
+// the other; device to host, every part's device copy is queued at once and
+// the threads copy each part out as soon as it has landed.
 #include <algorithm>
+#include <atomic>
 #include <condition_variable>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
+#include <memory>
 #include <mutex>
+#include <pthread.h>
 #include <system_error>
 #include <thread>
 #include <vector>
@@ -20,8 +27,8 @@
 namespace hos {
 namespace {
 
-constexpr size_t STAGE_MIN = 1u << 20;    // smaller copies go straight to the driver
-constexpr size_t PART_MIN = 256u << 10;   // smallest piece one copy thread takes
+constexpr size_t STAGE_MIN = 1u << 20;     // smaller copies go straight to the driver
+constexpr size_t WINDOW_MAX = 64u << 20;   // largest pinned buffer; longer copies go window by window
 
 int env_int(const char* name, int dflt) {
   const char* s = getenv(name);
@@ -29,38 +36,32 @@ int env_int(const char* name, int dflt) {
 }
 
 // ------------------------------------------------------------ copy threads
-// A job is a list of parts; every thread (the caller's included) claims the
-// next part under the lock, copies it without the lock and counts it done.
-// The pool lives until the process ends and its threads are detached: no
-// join at exit, and a process forked from this one (which has none of the
-// threads) still finishes every copy on the caller's thread.
+// A job is `nparts` parts, claimed in index order by the pool's threads and
+// by the caller's thread; work(k) does part k.
+// The caller's thread claims parts too, so a job finishes even with no copy
+// thread running.  The pool lives until the process ends and its threads
+// are detached: no join at exit; a process forked from this one has none of
+// the threads and starts its own.
 class CopyPool {
  public:
-  void copy(unsigned char* dst, const unsigned char* src, size_t bytes) {
-    const int nt = threads();
-    size_t parts = std::min<size_t>((size_t)nt, std::max<size_t>(1, bytes / PART_MIN));
-    if (parts <= 1) {
-      memcpy(dst, src, bytes);
-      return;
-    }
+  // In a forked child: the copy threads did not come along.
+  void forget_threads() { started_ = 0; }
+
+  void run(size_t nparts, const std::function<void(size_t)>& work) {
     std::lock_guard<std::mutex> job(job_m_);  // one job at a time
-    start(nt - 1);
-    size_t piece = (bytes + parts - 1) / parts;
-    piece = (piece + 4095) & ~(size_t)4095;
-    parts = (bytes + piece - 1) / piece;
+    start(threads() - 1);
+    unsigned long long g;
     {
       std::lock_guard<std::mutex> lk(m_);
-      dst_ = dst;
-      src_ = src;
-      bytes_ = bytes;
-      piece_ = piece;
-      nparts_ = parts;
+      work_ = &work;
+      nparts_ = nparts;
       next_ = 0;
       done_ = 0;
-      gen_++;
+      g = ++gen_;
     }
     cv_.notify_all();
-    work(gen_);
+    while (take_one(g)) {
+    }
     std::unique_lock<std::mutex> lk(m_);
     done_cv_.wait(lk, [&] { return done_ == nparts_; });
   }
@@ -74,17 +75,19 @@ class CopyPool {
     return nthreads_;
   }
 
-  void start(int workers) {
+  // Starts copy threads up to `workers`; returns how many run.
+  int start(int workers) {
     std::lock_guard<std::mutex> lk(m_);
     while (started_ < workers) {
       const unsigned long long g = gen_;
       try {
         std::thread([this, g] { loop(g); }).detach();
       } catch (const std::system_error&) {
-        return;  // no more threads: the caller's thread takes the parts
+        break;  // no more threads: the others take the parts
       }
       started_++;
     }
+    return started_;
   }
 
   [[noreturn]] void loop(unsigned long long seen) {
@@ -94,33 +97,30 @@ class CopyPool {
         cv_.wait(lk, [&] { return gen_ != seen; });
         seen = gen_;
       }
-      work(seen);
+      while (take_one(seen)) {
+      }
     }
   }
 
-  // Copies parts of job `g` until none is left (or a newer job replaced it).
-  void work(unsigned long long g) {
-    for (;;) {
-      unsigned char* d;
-      const unsigned char* s;
-      size_t n;
-      {
-        std::lock_guard<std::mutex> lk(m_);
-        if (gen_ != g || next_ >= nparts_) return;
-        const size_t off = next_ * piece_;
-        next_++;
-        d = dst_ + off;
-        s = src_ + off;
-        n = std::min(piece_, bytes_ - off);
-      }
-      memcpy(d, s, n);
-      bool last;
-      {
-        std::lock_guard<std::mutex> lk(m_);
-        last = ++done_ == nparts_;
-      }
-      if (last) done_cv_.notify_all();
+  // Claims and does one part of job g; false when none is left (or a newer
+  // job replaced it).
+  bool take_one(unsigned long long g) {
+    size_t k;
+    const std::function<void(size_t)>* w;
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      if (gen_ != g || next_ >= nparts_) return false;
+      k = next_++;
+      w = work_;
     }
+    (*w)(k);
+    bool last;
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      last = ++done_ == nparts_;
+    }
+    if (last) done_cv_.notify_all();
+    return true;
   }
 
   std::mutex job_m_;
@@ -129,33 +129,44 @@ class CopyPool {
   int started_ = 0;
   int nthreads_ = 0;
   unsigned long long gen_ = 0;
-  unsigned char* dst_ = nullptr;
-  const unsigned char* src_ = nullptr;
-  size_t bytes_ = 0, piece_ = 0, nparts_ = 0, next_ = 0, done_ = 0;
+  const std::function<void(size_t)>* work_ = nullptr;
+  size_t nparts_ = 0, next_ = 0, done_ = 0;
 };
 
+CopyPool* g_pool = nullptr;
+
 CopyPool& pool() {
-  static CopyPool* p = new CopyPool;  // never destroyed (see above)
+  static CopyPool* p = [] {
+    g_pool = new CopyPool;  // never destroyed (see above)
+    // a forked child has none of the parent's threads: it starts its own
+    pthread_atfork(nullptr, nullptr, [] { g_pool->forget_threads(); });
+    return g_pool;
+  }();
   return *p;
 }
 
-// ------------------------------------------------------------ staging buffers
+// ------------------------------------------------------------ staging buffer
 struct Stager {
   std::mutex m;
-  size_t chunk = 0;
-  unsigned char* pin[2] = {nullptr, nullptr};
-  bool failed = false;  // pinned allocation failed: copies go to the driver
-  std::vector<cudaEvent_t> ev;  // two per device, created on first use
+  unsigned char* pin = nullptr;  // pinned buffer of `cap` bytes
+  size_t cap = 0;
+  bool failed = false;           // pinned allocation failed: copies go to the driver
+  std::vector<std::vector<cudaEvent_t>> ev;  // per device: one per part of a window, created on first use
 };
 
 Stager& stager() {
-  static Stager* s = new Stager;  // lives until the process ends, like the pinned buffers
+  static Stager* s = new Stager;  // lives until the process ends, like the pinned buffer
   return *s;
 }
 
 bool staging_on() {
   static const int on = env_int("HOS_STAGE", 1);
   return on != 0;
+}
+
+size_t part_bytes() {
+  static const size_t p = (size_t)std::max(64, env_int("HOS_STAGE_CHUNK_KB", 1024)) << 10;
+  return p;
 }
 
 // Whether p is host memory the driver knows nothing about (pageable).
@@ -177,36 +188,34 @@ bool is_device(const void* p) {
   return a.type == cudaMemoryTypeDevice;
 }
 
-// The staging buffers and this device's two events (the caller holds s.m).
-cudaError_t prepare(Stager& s, cudaEvent_t* ev) {
-  if (!s.pin[0]) {
-    const int kb = std::max(64, env_int("HOS_STAGE_CHUNK_KB", 2048));
-    s.chunk = (size_t)kb << 10;
-    for (int b = 0; b < 2; b++) {
-      if (cudaHostAlloc((void**)&s.pin[b], s.chunk, cudaHostAllocPortable) != cudaSuccess) {
-        cudaGetLastError();
-        if (b == 1) cudaFreeHost(s.pin[0]);
-        s.pin[0] = s.pin[1] = nullptr;
-        s.failed = true;
-        return cudaErrorMemoryAllocation;
-      }
+// A pinned buffer for a copy of `bytes` (at most WINDOW_MAX) and `nparts`
+// events of the current device (the caller holds s.m; every earlier copy
+// through the buffer has finished).
+cudaError_t prepare(Stager& s, size_t bytes, size_t nparts, int* dev, cudaEvent_t** evs) {
+  const size_t need = std::min(bytes, WINDOW_MAX);
+  if (s.cap < need) {
+    if (s.pin) cudaFreeHost(s.pin);
+    s.pin = nullptr;
+    s.cap = 0;
+    if (cudaHostAlloc((void**)&s.pin, need, cudaHostAllocPortable) != cudaSuccess) {
+      cudaGetLastError();
+      s.pin = nullptr;
+      s.failed = true;
+      return cudaErrorMemoryAllocation;
     }
+    s.cap = need;
   }
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  cudaError_t e = cudaGetDevice(dev);
   if (e != cudaSuccess) return e;
-  if ((int)s.ev.size() < 2 * (dev + 1)) s.ev.resize(2 * (dev + 1), nullptr);
-  for (int b = 0; b < 2; b++) {
-    cudaEvent_t& x = s.ev[2 * dev + b];
-    if (!x) {
-      e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming);
-      if (e != cudaSuccess) {
-        x = nullptr;
-        return e;
-      }
-    }
-    ev[b] = x;
+  if ((int)s.ev.size() <= *dev) s.ev.resize(*dev + 1);
+  std::vector<cudaEvent_t>& v = s.ev[*dev];
+  while (v.size() < nparts) {
+    cudaEvent_t x;
+    e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming);
+    if (e != cudaSuccess) return e;
+    v.push_back(x);
   }
+  *evs = v.data();
   return cudaSuccess;
 }
 
@@ -216,54 +225,72 @@ cudaError_t prepare(Stager& s, cudaEvent_t* ev) {
     if (e_ != cudaSuccess) return e_;    \
   } while (0)
 
-// Pageable host -> device.  Each buffer is refilled only after the copy
-// engine has drained it; the last chunks are drained before returning so the
-// buffers are free for the next caller.
-cudaError_t staged_h2d(Stager& s, const cudaEvent_t* ev, unsigned char* dst, const unsigned char* src, size_t bytes,
-                       cudaStream_t st) {
-  const size_t C = s.chunk;
+// Pageable host -> device in chunks of two parts, through two halves of the
+// pinned buffer: all threads copy chunk i into one half (each a slice of it)
+// while the copy engine moves chunk i-1 out of the other.  (A part per thread
+// with the copy engine fed part by part measured slower: one thread's memcpy
+// is a fraction of the host's bandwidth.)  The last copies have finished when
+// the call returns, so the buffer is free for the next caller.
+cudaError_t staged_h2d(Stager& s, unsigned char* dst, const unsigned char* src, size_t bytes, cudaStream_t st) {
+  const size_t C = 2 * part_bytes();
+  int dev = 0;
+  cudaEvent_t* evs = nullptr;
+  ST_CK(prepare(s, std::max(bytes, 2 * C), 2, &dev, &evs));
   const size_t nch = (bytes + C - 1) / C;
   for (size_t i = 0; i < nch; i++) {
     const int b = (int)(i & 1);
+    unsigned char* half = s.pin + b * C;
     const size_t off = i * C, n = std::min(C, bytes - off);
-    if (i >= 2) ST_CK(cudaEventSynchronize(ev[b]));
-    pool().copy(s.pin[b], src + off, n);
-    ST_CK(cudaMemcpyAsync(dst + off, s.pin[b], n, cudaMemcpyHostToDevice, st));
-    ST_CK(cudaEventRecord(ev[b], st));
+    if (i >= 2) ST_CK(cudaEventSynchronize(evs[b]));
+    const size_t slice = std::max<size_t>(128u << 10, (n + 7) / 8);
+    const size_t nsl = (n + slice - 1) / slice;
+    const std::function<void(size_t)> work = [&](size_t k) {
+      const size_t o = k * slice;
+      memcpy(half + o, src + off + o, std::min(slice, n - o));
+    };
+    pool().run(nsl, work);
+    ST_CK(cudaMemcpyAsync(dst + off, half, n, cudaMemcpyHostToDevice, st));
+    ST_CK(cudaEventRecord(evs[b], st));
   }
-  for (size_t i = nch >= 2 ? nch - 2 : 0; i < nch; i++) ST_CK(cudaEventSynchronize(ev[i & 1]));
+  for (size_t i = nch >= 2 ? nch - 2 : 0; i < nch; i++) ST_CK(cudaEventSynchronize(evs[i & 1]));
   return cudaSuccess;
 }
 
-// Device -> pageable host: chunk i+1 is in flight while the host threads
-// copy chunk i out of the other buffer.
-cudaError_t staged_d2h(Stager& s, const cudaEvent_t* ev, unsigned char* dst, const unsigned char* src, size_t bytes,
-                       cudaStream_t st) {
-  const size_t C = s.chunk;
-  const size_t nch = (bytes + C - 1) / C;
-  auto issue = [&](size_t i) -> cudaError_t {
-    const int b = (int)(i & 1);
-    const size_t off = i * C, n = std::min(C, bytes - off);
-    cudaError_t e = cudaMemcpyAsync(s.pin[b], src + off, n, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaEventRecord(ev[b], st);
-    return e;
-  };
-  ST_CK(issue(0));
-  for (size_t i = 0; i < nch; i++) {
-    const int b = (int)(i & 1);
-    const size_t off = i * C, n = std::min(C, bytes - off);
-    if (i + 1 < nch) ST_CK(issue(i + 1));
-    ST_CK(cudaEventSynchronize(ev[b]));
-    pool().copy(dst + off, s.pin[b], n);
+// Device -> pageable host, window by window: every part's device copy is
+// queued first, each followed by an event; a thread that takes part k waits
+// for its event and copies it out while the later parts are still in flight.
+cudaError_t staged_d2h(Stager& s, unsigned char* dst, const unsigned char* src, size_t bytes, cudaStream_t st) {
+  const size_t P = part_bytes();
+  const size_t npmax = (std::min(bytes, WINDOW_MAX) + P - 1) / P;
+  int dev = 0;
+  cudaEvent_t* evs = nullptr;
+  ST_CK(prepare(s, bytes, npmax, &dev, &evs));
+  for (size_t w0 = 0; w0 < bytes; w0 += s.cap) {
+    const size_t wb = std::min(s.cap, bytes - w0);
+    const size_t np = (wb + P - 1) / P;
+    for (size_t k = 0; k < np; k++) {
+      const size_t off = k * P;
+      ST_CK(cudaMemcpyAsync(s.pin + off, src + w0 + off, std::min(P, wb - off), cudaMemcpyDeviceToHost, st));
+      ST_CK(cudaEventRecord(evs[k], st));
+    }
+    std::atomic<int> err{(int)cudaSuccess};
+    const std::function<void(size_t)> work = [&](size_t k) {
+      cudaError_t e = cudaSetDevice(dev);
+      if (e == cudaSuccess) e = cudaEventSynchronize(evs[k]);
+      if (e != cudaSuccess) {
+        err.store((int)e);
+        return;
+      }
+      const size_t off = k * P;
+      memcpy(dst + w0 + off, s.pin + off, std::min(P, wb - off));
+    };
+    pool().run(np, work);
+    if (err.load() != (int)cudaSuccess) return (cudaError_t)err.load();
   }
   return cudaSuccess;
 }
 
 }  // namespace
-
-void par_memcpy(void* dst, const void* src, size_t bytes) {
-  pool().copy(static_cast<unsigned char*>(dst), static_cast<const unsigned char*>(src), bytes);
-}
 
 cudaError_t host_copy(void* dst, const void* src, size_t bytes, cudaStream_t st) {
   if (bytes >= STAGE_MIN && staging_on()) {
@@ -272,11 +299,13 @@ cudaError_t host_copy(void* dst, const void* src, size_t bytes, cudaStream_t st)
     if (up || down) {
       Stager& s = stager();
       std::lock_guard<std::mutex> lk(s.m);
-      cudaEvent_t ev[2];
-      if (!s.failed && prepare(s, ev) == cudaSuccess) {
-        if (up)
-          return staged_h2d(s, ev, static_cast<unsigned char*>(dst), static_cast<const unsigned char*>(src), bytes, st);
-        return staged_d2h(s, ev, static_cast<unsigned char*>(dst), static_cast<const unsigned char*>(src), bytes, st);
+      if (!s.failed) {
+        cudaError_t e = up ? staged_h2d(s, static_cast<unsigned char*>(dst), static_cast<const unsigned char*>(src),
+                                        bytes, st)
+                           : staged_d2h(s, static_cast<unsigned char*>(dst), static_cast<const unsigned char*>(src),
+                                        bytes, st);
+        if (e != cudaErrorMemoryAllocation || !s.failed) return e;
+        // the pinned buffer could not be had: the driver's path below
       }
     }
   }

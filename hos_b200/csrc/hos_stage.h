@@ -1,10 +1,11 @@
 // Copies between the caller's host arrays and the device.
 //
 // A large array in pageable host memory (what fftw_alloc / malloc return,
-// and what the reference's driver hands to sol_update_RK) is moved through
-// two pinned staging buffers: host threads copy chunk i into one buffer
-// while the copy engine moves chunk i-1 out of the other.  Pinned host
-// memory, device memory and small arrays go straight to cudaMemcpyAsync.
+// and what the reference's driver hands to sol_update_RK) is moved through a
+// pinned staging buffer in parts: host threads copy the parts, and each part
+// crosses to or from the device while the threads work on the next ones.
+// Pinned host memory, device memory and small arrays go straight to
+// cudaMemcpyAsync.
 #pragma once
 
 #include <cstddef>
@@ -18,9 +19,5 @@ namespace hos {
 // pageable host memory has read all of src when this returns; a staged copy
 // into pageable host memory has written all of dst when this returns.
 cudaError_t host_copy(void* dst, const void* src, size_t bytes, cudaStream_t st);
-
-// Host memcpy split over the library's copy threads (the caller's thread
-// takes parts too, so it finishes even if no copy thread is running).
-void par_memcpy(void* dst, const void* src, size_t bytes);
 
 }  // namespace hos

@@ -62,6 +62,7 @@ class Request:
     seed: int = 0
     precision: str = "fp32"
     # filled by the server
+    steps_done: int = 0  # steps taken so far (all of them once done)
     admitted: float | None = None
     finished: float | None = None
     status: str = "queued"  # queued, active, done, failed, cancelled, rejected
@@ -614,6 +615,7 @@ class Server:
                     took = a[3] - left
                     chunk_gp += took * a[0].n * a[0].n
                     a[3] = left
+                    a[0].steps_done = a[0].steps - left
                 gp_steps += chunk_gp
                 if chunk_gp > 0 and chunk_s > 0:
                     self.rate = 0.7 * self.rate + 0.3 * (chunk_gp / chunk_s)

@@ -96,7 +96,7 @@ def test_every_request_gets_exactly_its_steps():
     m = Server(chunk=4, reserve_bytes=0, backend=be).run(rs, realtime=False)
     assert m["completed"] == 7 and m["submitted"] == 7
     for r in rs:
-        assert r.status == "done" and r.result == (r.steps,)
+        assert r.status == "done" and r.result == (r.steps,) and r.steps_done == r.steps
     assert be.held == 0 and all(f.closed for f in be.opened)
 
 
