@@ -755,7 +755,7 @@ def run_ours(args, rep):
                           "(Csource/2dpar hot-path sources with the single-rank FFTW-MPI shim)",
             }
     dropin = run_legacy(args, eta, phi, dt)
-    # the figures the configurations are judged on, last so that a reader of
+    # the figures that describe the configurations, last so that a reader of
     # the line's tail sees them
     line["dropin"] = dropin
     line["fp64"] = {"value": v64, "ms_per_step": timings["fp64"] / args.steps}
