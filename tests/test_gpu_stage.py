@@ -55,3 +55,27 @@ def test_staged_copies_match_direct_copies(tmp_path):
     np.testing.assert_array_equal(staged["back"], staged["u"])
     for k in ("back", "r", "pe", "pp", "s3"):
         np.testing.assert_array_equal(staged[k], direct[k], err_msg=k)
+
+
+CHILD_LARGE = r"""
+import sys
+import numpy as np
+from hos_b200.field import HosField
+out = sys.argv[1]
+n = 2048  # the packed state is 67 MB: more than one window of the 64 MB staging buffer
+f = HosField(n, n, order=3)
+rng = np.random.default_rng(11)
+shape = (2, n // 2 + 1, n)
+u = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+f.set_state_spectral(u, 0.0)
+back, _ = f.state_spectral()
+np.savez(out, ok=np.array([np.array_equal(back, u)]))
+"""
+
+
+def test_staged_copies_longer_than_the_staging_buffer(tmp_path):
+    out = os.path.join(str(tmp_path), "large.npz")
+    p = subprocess.run([sys.executable, "-c", CHILD_LARGE, out], env=dict(os.environ, PYTHONPATH=ROOT), cwd=ROOT,
+                       capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr[-2000:]
+    assert bool(np.load(out)["ok"][0])
