@@ -155,8 +155,11 @@ class DeviceBackend:
         from . import _lib
 
         out = ctypes.c_size_t()
-        _lib_check(_lib.load().hos_device_free_bytes(ctypes.byref(out)))
-        return int(out.value)
+        if _lib.load().hos_device_free_bytes(ctypes.byref(out)) == 0:
+            return int(out.value)
+        import torch  # the pool's figures are not available: the driver's free memory
+
+        return torch.cuda.mem_get_info()[0]
 
     def open(self, r):
         """Creates the request's field with its initial sea; returns (field, dt)."""
